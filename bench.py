@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""MM-GBSA throughput on B200: frames/s of the batched, binding-fused engine.
+
+Workload (default): synthetic receptor of 5,000 atoms + 50-atom ligand
+(receptor residues of 15 atoms), 1,000 frames (sigma 0.5 A), OBC-II GB with
+eps 1/78.5, 0.15 M salt, no cutoff, SASA with 960 points per atom, and
+per-residue decomposition of every frame.  One step = one pass of the engine
+over the 1,000 frames.
+
+Reported (one JSON line on rank 0):
+  value      frames/s, frames resident in HBM, device time of K steps
+             (CUDA events on the library's stream), max over ranks
+  e2e        frames/s through BindingSystem.run with pinned host frames:
+             host->device copy of the frames and device->host copy of the
+             per-frame energies and per-residue terms inside the timed region
+  plain_gpu  frames/s of the plain FP64 form (one subsystem per launch
+             sequence, per frame) on a sample of frames
+  roofline   dominant kernel: algorithmic FLOPs / its CUDA-event duration vs
+             the measured FP32 FMA peak of this GPU
+  cpu_baseline  the CPU restatement of the reference (all host threads) on a
+             bounded sample of the same frames
+  serving    p50 / p99 request latency and frames/s of a bounded mixed
+             request stream through the serving loop
+With --gpus N each rank runs its own 1,000 frames (weak scaling, replicas:
+the path has no exchange step).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rust-simulation-tools_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "MM-GBSA frames/s (batched, binding-fused, mixed precision)"
+GB = dict(model=2, solvent_dielectric=78.5, salt_concentration=0.15)
+NPTS = 960
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def workload(n_frames, rank):
+    from rust_simulation_tools import synthetic as S
+
+    s = S.make_system(5000, 50, seed=1002)
+    fr = S.make_frames(s, n_frames, seed=2002 + 7919 * rank)
+    return s, fr
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device):
+        self.device, self.rows, self.proc = device, [], None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) > 8 for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline(s, fr, n_sample):
+    import oracle as O
+
+    O.build()
+    d = tempfile.mkdtemp()
+    from rust_simulation_tools import synthetic as S
+
+    S.write_prmtop(s, os.path.join(d, "w.prmtop"))
+    top = O.Topology.load(os.path.join(d, "w.prmtop"))
+    x = (fr[:n_sample].astype(np.float64) * 0.1) * 10.0
+    gb = O.gb_params("obc2", solvent_dielectric=78.5)
+    sa = O.sa_params(n_points=NPTS)
+    t = time.perf_counter()
+    O.binding_frames(top, x, s.receptor_residues, s.ligand_residues, gb=gb, sa=sa)
+    for f in range(n_sample):  # decomposition of every frame, as the GPU step does
+        O.decompose(top, x[f], s.receptor_residues, s.ligand_residues, gb, sa)
+    dt = time.perf_counter() - t
+    return {"value": n_sample / dt, "unit": "frames/s", "cores": O.threads(), "kind": "port",
+            "sample": f"{n_sample} frames of the 5,050-atom workload, binding frame + decomposition, "
+                      f"C++ restatement of the reference, {O.threads()} OpenMP threads"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    s, fr = workload(max(args.ref_frames, 1), 0)
+    samples = []
+    for k in range(args.warmup + args.steps):
+        r = cpu_baseline(s, fr, args.ref_frames)
+        if k >= args.warmup:
+            samples.append(r["value"])
+    v = float(np.median(samples))
+    line = {"metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * args.ref_frames / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "MM-GBSA + per-residue decomposition, 5,000 + 50 atoms, 1,000 frames",
+                       "sample_frames_per_step": args.ref_frames},
+            "cpu_baseline": {"value": v, "unit": "frames/s", "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def serving_stream(rst, ctx, n_req, seed=4):
+    """Bounded mixed stream: receptors log-uniform 1k-20k atoms, ligands
+    20-80 atoms, 1-200 frames per request, Poisson arrivals."""
+    from rust_simulation_tools import synthetic as S
+
+    rng = np.random.default_rng(seed)
+    d = tempfile.mkdtemp()
+    systems = []
+    for k in range(6):
+        nr = int(round(np.exp(rng.uniform(np.log(1000), np.log(20000)))))
+        nl = int(rng.integers(20, 81))
+        s = S.make_system(nr, nl, seed=3000 + k)
+        p = os.path.join(d, f"s{k}.prmtop")
+        S.write_prmtop(s, p)
+        top = rst.read_prmtop(p)
+        bs = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, gb_params=rst.GbParams(**GB),
+                               sa_params=rst.SaParams(n_sphere_points=NPTS), ctx=ctx)
+        systems.append((s, bs))
+    reqs = []
+    for _ in range(n_req):
+        k = int(rng.integers(0, len(systems)))
+        reqs.append((k, S.make_frames(systems[k][0], int(rng.integers(1, 201)), seed=int(rng.integers(1 << 30)))))
+    for k, (s, bs) in enumerate(systems):  # first-use preparation outside the stream
+        bs.run(S.make_frames(s, 1, seed=1))
+    srv = rst.Server(max_inflight=4, ctx=ctx)
+    gaps = rng.exponential(0.01, size=n_req)
+    t0 = time.perf_counter()
+    ids = []
+    for (k, fr), g in zip(reqs, gaps):
+        time.sleep(g)
+        ids.append(srv.submit(systems[k][1], fr))
+    for i in ids:
+        srv.wait(i, 600000)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    frames = sum(fr.shape[0] for _, fr in reqs)
+    return {"requests": n_req, "frames": frames, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "frames_per_s": frames / wall, "arrival_mean_ms": 10.0}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=1000)
+    ap.add_argument("--ref-frames", type=int, default=8)
+    ap.add_argument("--plain-frames", type=int, default=16)
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e/plain/cpu/serving legs")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    rank, world, local = dist_env()
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    torch.cuda.set_device(local)
+    import rust_simulation_tools as rst
+    from rust_simulation_tools import _native as N
+
+    stream = torch.cuda.current_stream()
+    ctx = N.make_ctx(local, stream.cuda_stream)
+    s, fr = workload(args.frames, rank)
+    d = tempfile.mkdtemp()
+    from rust_simulation_tools import synthetic as S
+
+    S.write_prmtop(s, os.path.join(d, "w.prmtop"))
+    top = rst.read_prmtop(os.path.join(d, "w.prmtop"))
+    gb, sa = rst.GbParams(**GB), rst.SaParams(n_sphere_points=NPTS)
+    sysf = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, gb_params=gb, sa_params=sa, ctx=ctx)
+    F, nres = fr.shape[0], sysf.n_residues
+    d_fr = torch.from_numpy(fr).cuda()
+    d_out = torch.empty((F, 13), dtype=torch.float64, device="cuda")
+    d_dec = torch.empty((F, nres, 4), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        sysf.run_device(d_fr.data_ptr(), F, d_out.data_ptr(), d_dec.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = int(N.lib.rstg_ctx_kernel_launches(ctx))
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for a, b in evs:
+            flush.zero_()  # L2 flush between timed steps (outside the events)
+            a.record(stream)
+            step()
+            b.record(stream)
+        torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    launches = int(N.lib.rstg_ctx_kernel_launches(ctx)) - launches0
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    if pg:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * F * args.steps / (ms / 1000.0)
+    stats = sysf.last_stats()
+    out_np = d_out.cpu().numpy()
+
+    extras = {}
+    if not args.no_extras:
+        # end to end through the public API with pinned host buffers
+        h_fr = torch.from_numpy(fr).pin_memory().numpy()
+        sysf.run(h_fr, decompose=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        res, dec = sysf.run(h_fr, decompose=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+        if pg:
+            t = torch.tensor([e2e_ms], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        extras["e2e"] = {"value": world * F / (e2e_ms / 1000.0), "unit": "frames/s",
+                         "h2d_bytes_per_step": int(fr.nbytes), "d2h_bytes_per_step": int(res.nbytes + dec.nbytes)}
+        assert np.array_equal(res, out_np), "host and device paths disagree"
+        # per-kernel roofline
+        import ctypes as C
+
+        n = C.c_int32()
+        names = C.create_string_buffer(8 * 32)
+        kms, kfl, kby = np.zeros(8), np.zeros(8), np.zeros(8)
+        N.check(N.lib.rstg_system_profile(sysf._h, N.vp(d_fr.data_ptr()), F, C.byref(n), names,
+                                          kms.ctypes.data_as(C.POINTER(C.c_double)),
+                                          kfl.ctypes.data_as(C.POINTER(C.c_double)),
+                                          kby.ctypes.data_as(C.POINTER(C.c_double))))
+        kn = [names.raw[32 * k:32 * k + 32].split(b"\0")[0].decode() for k in range(n.value)]
+        cal = np.zeros(4)
+        N.check(N.lib.rstg_calibrate(local, cal.ctypes.data_as(C.POINTER(C.c_double))))
+        tot = kms[:n.value].sum()
+        share = {kn[k]: round(float(kms[k] / tot), 4) for k in range(n.value)}
+        top_k = int(np.argmax(kms[:n.value]))
+        fl_k = max(int(np.argmax(np.where(kfl[:n.value] > 0, kms[:n.value], -1))), 0)
+        ach = kfl[fl_k] / (kms[fl_k] / 1000.0) / 1e12
+        extras["roofline"] = {"bound": "fp32", "kernel": kn[fl_k], "achieved": ach, "peak": float(cal[0]),
+                              "unit": "TFLOP/s", "frac": ach / cal[0], "traffic": None,
+                              "peak_source": "measured FP32 FMA loop (rstg_calibrate) on this GPU",
+                              "dominant_kernel": kn[top_k], "kernel_share": share,
+                              "kernel_ms_per_1000_frames": {kn[k]: round(float(kms[k]) * 1000.0 / F, 3)
+                                                            for k in range(n.value)},
+                              "fp64_fma_tflops": float(cal[1]), "mufu_ex2_gops": float(cal[2]),
+                              "sm_max_mhz_attr": float(cal[3])}
+        # plain FP64 GPU form on a sample
+        if args.plain_frames > 0:
+            sysp = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, gb_params=gb, sa_params=sa,
+                                     mode="plain", ctx=ctx)
+            sysp.run(fr[:1], decompose=True)
+            t = time.perf_counter()
+            sysp.run(fr[:args.plain_frames], decompose=True)
+            pv = args.plain_frames / (time.perf_counter() - t)
+            extras["plain_gpu"] = {"value": pv, "unit": "frames/s", "sample_frames": args.plain_frames,
+                                   "form": "FP64, one subsystem per launch sequence, per frame, decomposition"}
+            extras["speedup_vs_plain_gpu"] = value / world / pv
+        if rank == 0 and world == 1 and args.ref_frames > 0:
+            extras["cpu_baseline"] = cpu_baseline(s, fr, args.ref_frames)
+        if rank == 0 and world == 1 and args.serve_requests > 0:
+            extras["serving"] = serving_stream(rst, ctx, args.serve_requests)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 pairs, f64 reductions",
+                "data": "synthetic (seeded generator, 0.12 atoms/A^3, sigma 0.5 A frames)",
+                "config": {"workload": "MM-GBSA + per-residue decomposition, receptor 5,000 + ligand 50 atoms, "
+                                       "335 residues, 1,000 frames per GPU",
+                           "gb": "OBC-II eps 1/78.5 0.15 M no cutoff", "sasa_points": NPTS,
+                           "frames_per_gpu": F, "l2": "256 MB flush between timed steps",
+                           "parallelism": f"replicas x{world} (frames sharded, no exchange)"},
+                "gpu_launches": launches, "clocks": clk.summary(),
+                "precision_stats": stats}
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1283 @@
+// Batched, binding-difference-fused MM-GBSA engine.
+//
+// Layout: complex atoms are permuted into "slots": receptor atoms first
+// (slots [0, nR)), then ligand atoms (slots [nR, nC)); each part is sorted
+// along a Morton curve of the first frame so that a 128-slot tile is a compact
+// blob and close pairs fall into few tiles.  Per batch of B frames:
+//
+//   K0 prep     input frames -> slot-ordered FP64 and FP32 coordinates
+//   K1 psi      HCT descreening over all ordered complex pairs, split into
+//               own-part and other-part sums: psi_C = psi_own + psi_other
+//               (descreening is pairwise additive, gb_energy.rs:157-217), so
+//               the complex and sub-system Born radii come from one pass;
+//               also emits each atom's SASA neighbour list
+//   K2 pairs    triangular 128x128 tiles: GB pair energy with complex radii
+//               and, for same-part pairs, with sub-system radii; LJ+Coulomb
+//               for same-part pairs
+//   K3 sasa     one warp per atom: a point is accessible in the sub-system iff
+//               no own-part neighbour buries it, and in the complex iff also
+//               no other-part neighbour does (core/src/sasa.rs:256-265)
+//   K4 rl       receptor x ligand LJ+Coulomb in FP64, per-atom row/column sums
+//               (binding difference of the non-bonded term and the
+//               per-residue vdW/elec of decomposition.rs:240-283)
+//   K6 bonded   bonded terms by part, and 1-4 class corrections
+//   K5 reduce   per-frame FrameEnergy (binding.rs:333-415) and per-residue
+//               terms (decomposition.rs:309-375)
+//
+// Precision: FP32 pair arithmetic with FP64 accumulation; close pairs
+// (r < 3.5 A for LJ/Coulomb, any pair outside the far-field series domain for
+// the HCT integral) take the reference's FP64 expressions; SASA point tests
+// are FP32 with an FP64 re-check of the reference expression inside a
+// +-2e-4 A^2 band, so accessible-point counts equal the reference's.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <unordered_map>
+
+#include "common.cuh"
+#include "system.hpp"
+
+namespace rstg {
+
+static constexpr float kSasaBand = 2e-4f;  // A^2, FP32 error bound x 10
+static constexpr float kNbGuard2 = 3.5f * 3.5f;
+static constexpr int kSasaWarps = 4;
+
+struct GbConstF {
+  double kappa, inv_ein, inv_eout, diel_ns, cut2;
+  float fk, fie, fio, fdns, fcut2;
+  int no_salt, model;
+  double rgbmax;
+};
+
+struct FusedParams {
+  DevBuf slot_src, P32, q64, rho64, rad64, sj64, type, lj32, lj64, tiles, tile_rec, masks, sphere32, sphere64,
+      res_ptr, res_slots, bterms, bpar, corr;
+  int nt = 0, nb = 0, ntiles = 0, nrec = 0, npts = 0, nres = 0, nterms = 0, ncorr = 0;
+  double probe = 1.4;
+  GbConstF gb{};
+};
+
+// ---------------------------------------------------------------------------
+// K0: prep
+// ---------------------------------------------------------------------------
+__global__ void k_prep(int nC, int n_top, const void* __restrict__ in, int f64, const int* __restrict__ slot_src,
+                       const float4* __restrict__ P32, double* __restrict__ xyz64, float4* __restrict__ xyz32) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  int f = blockIdx.y;
+  if (s >= nC) return;
+  long long src = ((long long)f * n_top + slot_src[s]) * 3;
+  double x[3];
+  if (f64) {
+    const double* p = (const double*)in + src;
+    x[0] = p[0];
+    x[1] = p[1];
+    x[2] = p[2];
+  } else {
+    // DCD path: float32 Angstrom -> f64 nm (dcd.rs:429-437) -> Angstrom (binding.rs:630-633)
+    const float* p = (const float*)in + src;
+    for (int d = 0; d < 3; d++) x[d] = __dmul_rn(__dmul_rn((double)p[d], 0.1), 10.0);
+  }
+  long long o = (long long)f * nC + s;
+  xyz64[3 * o] = x[0];
+  xyz64[3 * o + 1] = x[1];
+  xyz64[3 * o + 2] = x[2];
+  xyz32[o] = make_float4((float)x[0], (float)x[1], (float)x[2], P32[s].x);
+}
+
+// ---------------------------------------------------------------------------
+// K1: psi + Born radii + self energies + SASA neighbour lists
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double hct64(double r2, double rho_i, double sj, bool& used) {
+  double r = sqrt(r2);
+  used = false;
+  if (r == 0.0 || rho_i >= r + sj) return 0.0;
+  double u = r + sj;
+  double l = (rho_i > fabs(r - sj)) ? rho_i : fabs(r - sj);
+  double l_inv = 1.0 / l, u_inv = 1.0 / u;
+  double c = 0.5 * (l_inv - u_inv + 0.25 * (u_inv * u_inv - l_inv * l_inv) * (r - sj * sj / r) + log(l / u) / (2.0 * r));
+  used = true;
+  return (rho_i < sj - r) ? c + 2.0 * (1.0 / rho_i - l_inv) : c;
+}
+
+__device__ __forceinline__ double radius64(double psi, double rho_i, double radius_i, int model, double rgbmax) {
+  double alpha = 1.0, beta = 0.0, gamma = 0.0;
+  if (model == 1) {
+    alpha = 0.8;
+    gamma = 2.909125;
+  } else if (model == 2) {
+    beta = 0.8;
+    gamma = 4.85;
+  }
+  double R;
+  if (model == 0) {
+    double inv_r = 1.0 / rho_i - psi;
+    R = inv_r > 0.0 ? 1.0 / inv_r : rgbmax;
+  } else {
+    double pr = psi * rho_i, p2 = pr * pr, p3 = p2 * pr;
+    double inv_r = 1.0 / rho_i - tanh(alpha * pr - beta * p2 + gamma * p3) / radius_i;
+    R = inv_r > 0.0 ? 1.0 / inv_r : rgbmax;
+  }
+  return R > rgbmax ? rgbmax : R;
+}
+
+__device__ __forceinline__ double self64(double q, double R, const GbConstF& k) {
+  if (k.no_salt) return k.diel_ns * q * q / R;
+  return -0.5 * q * q * (k.inv_ein - exp(-kKScale * k.kappa * R) * k.inv_eout) / R;
+}
+
+// Far-field HCT integral: with l = r - s, u = r + s (rho_i <= r - s) the
+// reference expression equals (1/r) sum_k k/(2k+1) x^(2k+1), x = s/r.  The
+// series has no cancellation; truncated after k = 6 it is exact to 1e-8
+// relative for x <= 1/4.
+__device__ __forceinline__ float hct_far(float x, float rinv) {
+  float x2 = x * x;
+  float p = fmaf(x2, 6.0f / 13.0f, 5.0f / 11.0f);
+  p = fmaf(x2, p, 4.0f / 9.0f);
+  p = fmaf(x2, p, 3.0f / 7.0f);
+  p = fmaf(x2, p, 2.0f / 5.0f);
+  p = fmaf(x2, p, 1.0f / 3.0f);
+  return x * x2 * rinv * p;
+}
+
+__global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __restrict__ xyz32,
+                                               const double* __restrict__ xyz64, const float4* __restrict__ P32,
+                                               const double* __restrict__ rho64, const double* __restrict__ sj64,
+                                               const double* __restrict__ rad64, const double* __restrict__ q64,
+                                               GbConstF k, float probe, int cap, int* __restrict__ nbr,
+                                               int* __restrict__ nbrcnt, double* __restrict__ R64,
+                                               float4* __restrict__ Rf, double* __restrict__ part,
+                                               int* __restrict__ diag) {
+  __shared__ float4 sx[kTile];
+  __shared__ float2 sp[kTile];
+  __shared__ double sh[32];
+  int f = blockIdx.y, i = blockIdx.x * kTile + threadIdx.x;
+  bool valid = i < nC;
+  const float4* X = xyz32 + (long long)f * nC;
+  const double* X64 = xyz64 + (long long)f * nC * 3;
+  float4 xi = valid ? X[i] : make_float4(0, 0, 0, 0);
+  float4 pi = valid ? P32[i] : make_float4(0, 0, 0, 0);
+  float rho_i = pi.y, ext_i = pi.w;
+  double rho_i64 = valid ? rho64[i] : 0.0;
+  bool in_r = i < nR;
+  double psi_own = 0.0, psi_oth = 0.0;
+  int cnt = 0, near64 = 0;
+  int* my = nbr + ((long long)f * nC + (valid ? i : 0)) * cap;
+  for (int j0 = 0; j0 < nC; j0 += kTile) {
+    int jl = j0 + threadIdx.x;
+    if (jl < nC) {
+      sx[threadIdx.x] = X[jl];
+      float4 pj = P32[jl];
+      sp[threadIdx.x] = make_float2(pj.z, pj.w);
+    }
+    __syncthreads();
+    int m = min(kTile, nC - j0);
+    float po = 0.f, pc = 0.f;
+    if (valid) {
+      for (int jj = 0; jj < m; jj++) {
+        int j = j0 + jj;
+        float4 xj = sx[jj];
+        float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        float2 s = sp[jj];
+        float ee = ext_i + s.y;
+        if (j != i && r2 <= fmaf(ee * ee, 1.00001f, 1e-4f)) {
+          if (cnt < cap) my[cnt] = j;
+          cnt++;
+        }
+        if (j == i || r2 > k.fcut2) continue;
+        float rinv = rsqrtf(r2), r = r2 * rinv, sj = s.x;
+        bool own = (j < nR) == in_r;
+        if (r2 > 0.f && 16.f * sj * sj <= r2 && rho_i <= r - sj) {
+          float t = hct_far(sj * rinv, rinv);
+          if (own)
+            po += t;
+          else
+            pc += t;
+        } else {
+          near64++;
+          double ddx = X64[3 * i] - X64[3 * j], ddy = X64[3 * i + 1] - X64[3 * j + 1],
+                 ddz = X64[3 * i + 2] - X64[3 * j + 2];
+          double rr2 = ddx * ddx + ddy * ddy + ddz * ddz;
+          if (rr2 > k.cut2) continue;
+          bool used;
+          double t = hct64(rr2, rho_i64, sj64[j], used);
+          if (used) {
+            if (own)
+              psi_own += t;
+            else
+              psi_oth += t;
+          }
+        }
+      }
+    }
+    psi_own += (double)po;
+    psi_oth += (double)pc;
+    __syncthreads();
+  }
+  double sC = 0.0, sR = 0.0, sL = 0.0, sD = 0.0;
+  if (valid) {
+    nbrcnt[(long long)f * nC + i] = cnt;
+    if (cnt > cap) atomicMax(diag + 3, cnt);
+    double Rc = radius64(psi_own + psi_oth, rho_i64, rad64[i], k.model, k.rgbmax);
+    double Rs = radius64(psi_own, rho_i64, rad64[i], k.model, k.rgbmax);
+    long long o = (long long)f * nC + i;
+    R64[2 * o] = Rc;
+    R64[2 * o + 1] = Rs;
+    Rf[o] = make_float4((float)Rc, (float)Rs, (float)(1.0 / Rc), (float)(1.0 / Rs));
+    double q = q64[i], ec = self64(q, Rc, k), es = self64(q, Rs, k);
+    sC = ec;
+    sD = ec - es;
+    if (in_r)
+      sR = es;
+    else
+      sL = es;
+  }
+  if (near64) atomicAdd((unsigned long long*)(diag + 4), (unsigned long long)near64);
+  sC = block_sum(sC, sh);
+  sR = block_sum(sR, sh);
+  sL = block_sum(sL, sh);
+  sD = block_sum(sD, sh);
+  if (threadIdx.x == 0) {
+    double* p = part + ((long long)f * gridDim.x + blockIdx.x) * 4;
+    p[0] = sC;
+    p[1] = sR;
+    p[2] = sL;
+    p[3] = sD;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K2: pair energies on triangular tiles
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float gb_pair32(float qq, float r2, float RiRj, float t, const GbConstF& k) {
+  // f_GB = sqrt(r2 + RiRj exp(-r2 / (4 RiRj))) (gb_energy.rs:339-346); t = r2 / (4 RiRj)
+  float e = t < 16.f ? __expf(-t) : 0.f;
+  float f2 = fmaf(RiRj, e, r2);
+  float finv = rsqrtf(f2);
+  if (k.no_salt) return k.fdns * qq * finv;
+  float f = f2 * finv;
+  return -0.5f * qq * (k.fie - __expf(-k.fk * f) * k.fio) * finv;
+}
+
+__device__ __forceinline__ double nb64(const double* X64, int i, int j, double qq, double A, double B, int cls,
+                                      double scee, double scnb) {
+  double dx = X64[3 * i] - X64[3 * j], dy = X64[3 * i + 1] - X64[3 * j + 1], dz = X64[3 * i + 2] - X64[3 * j + 2];
+  double r2 = dx * dx + dy * dy + dz * dz, r = sqrt(r2), r6 = r2 * r2 * r2, r12 = r6 * r6;
+  if (cls == 2) return (A / r12 - B / r6) / scnb + qq / r / scee;
+  return (A / r12 - B / r6) + qq / r;
+}
+
+struct PairOut {
+  double gbC, gbR, gbL, dgb, mmR, mmL;
+};
+
+__global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __restrict__ tiles,
+                                                 const float4* __restrict__ xyz32, const double* __restrict__ xyz64,
+                                                 const float4* __restrict__ Rf, const int* __restrict__ type, int nt,
+                                                 const float2* __restrict__ lj32, const double2* __restrict__ lj64,
+                                                 const unsigned* __restrict__ masks, GbConstF k, double scee,
+                                                 double scnb, double* __restrict__ part, int* __restrict__ diag) {
+  extern __shared__ float2 slj[];  // nt*nt (A, B)
+  __shared__ float4 sx[kTile];
+  __shared__ float4 sR[kTile];
+  __shared__ int st[kTile];
+  __shared__ double sh[32];
+  for (int t = threadIdx.x; t < nt * nt; t += blockDim.x) slj[t] = lj32[t];
+  int4 tl = tiles[blockIdx.x];
+  int f = blockIdx.y, bi = tl.x, bj = tl.y, rec = tl.z;
+  int i = bi * kTile + threadIdx.x, j0 = bj * kTile;
+  const float4* X = xyz32 + (long long)f * nC;
+  const double* X64 = xyz64 + (long long)f * nC * 3;
+  const float4* RF = Rf + (long long)f * nC;
+  int jl = j0 + threadIdx.x;
+  if (jl < nC) {
+    sx[threadIdx.x] = X[jl];
+    sR[threadIdx.x] = RF[jl];
+    st[threadIdx.x] = type[jl];
+  }
+  __syncthreads();
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  int n64 = 0;
+  if (i < nC) {
+    float4 xi = X[i];
+    float4 Ri = RF[i];
+    int ti = type[i];
+    bool in_r = i < nR;
+    float iRc = Ri.z, iRs = Ri.w;
+    unsigned mex[4] = {0, 0, 0, 0}, m14[4] = {0, 0, 0, 0};
+    if (rec >= 0) {
+      const unsigned* mr = masks + ((long long)rec * 2 * kTile + threadIdx.x) * 4;
+      for (int w = 0; w < 4; w++) {
+        mex[w] = mr[w];
+        m14[w] = mr[kTile * 4 + w];
+      }
+    }
+    int m = min(kTile, nC - j0);
+    int jstart = (bi == bj) ? threadIdx.x + 1 : 0;
+    for (int c0 = jstart; c0 < m; c0 += 32) {
+      float a[6] = {0, 0, 0, 0, 0, 0};
+      int cend = min(m, c0 + 32);
+      for (int jj = c0; jj < cend; jj++) {
+        int j = j0 + jj;
+        float4 xj = sx[jj];
+        float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (r2 > k.fcut2) continue;
+        float4 Rj = sR[jj];
+        float qq = xi.w * xj.w;
+        bool same = (j < nR) == in_r;
+        float iRcj = Rj.z;
+        float tc = 0.25f * r2 * iRc * iRcj;
+        float pC = gb_pair32(qq, r2, Ri.x * Rj.x, tc, k);
+        a[0] += pC;
+        if (same) {
+          float iRsj = Rj.w;
+          float ts = 0.25f * r2 * iRs * iRsj;
+          float pS = (tc >= 16.f && ts >= 16.f) ? pC : gb_pair32(qq, r2, Ri.y * Rj.y, ts, k);
+          a[in_r ? 1 : 2] += pS;
+          a[3] += pC - pS;
+          int cls = 1;
+          if (rec >= 0) {
+            int w = jj >> 5, b = jj & 31;
+            if ((m14[w] >> b) & 1u)
+              cls = 2;
+            else if ((mex[w] >> b) & 1u)
+              cls = 0;
+          }
+          if (cls) {
+            int tj = st[jj];
+            if (r2 < kNbGuard2 || cls == 2) {
+              double2 ab = lj64[ti * nt + tj];
+              double e = nb64(X64, i, j, (double)qq, ab.x, ab.y, cls, scee, scnb);
+              acc[in_r ? 4 : 5] += e;
+              n64++;
+            } else {
+              float2 ab = slj[ti * nt + tj];
+              float rinv = rsqrtf(r2), ir2 = rinv * rinv, ir6 = ir2 * ir2 * ir2;
+              a[in_r ? 4 : 5] += fmaf(ab.x * ir6, ir6, fmaf(-ab.y, ir6, qq * rinv));
+            }
+          }
+        } else {
+          a[3] += pC;
+        }
+      }
+      for (int q = 0; q < 6; q++) acc[q] += (double)a[q];
+    }
+  }
+  if (n64) atomicAdd((unsigned long long*)(diag + 4), (unsigned long long)n64);
+  double* p = part + ((long long)f * gridDim.x + blockIdx.x) * 6;
+  for (int q = 0; q < 6; q++) {
+    double v = block_sum(acc[q], sh);
+    if (threadIdx.x == 0) p[q] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K3: SASA (one warp per atom), own-part then other-part neighbours
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool exact_buried(const double* X64, int i, int j, const double* sph64, int p, double er,
+                                             double oer) {
+  // core/src/sasa.rs:249-265 with explicit single roundings
+  double t[3], d2 = 0.0;
+  for (int d = 0; d < 3; d++) t[d] = __dadd_rn(X64[3 * i + d], __dmul_rn(sph64[3 * p + d], er));
+  double dx = __dsub_rn(t[0], X64[3 * j]), dy = __dsub_rn(t[1], X64[3 * j + 1]), dz = __dsub_rn(t[2], X64[3 * j + 2]);
+  d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  return !(d2 > __dmul_rn(oer, oer));
+}
+
+__global__ void k_sasa(int nC, int nR, int cap, const int* __restrict__ nbr, const int* __restrict__ nbrcnt,
+                       const float4* __restrict__ xyz32, const double* __restrict__ xyz64,
+                       const double* __restrict__ rad64, double probe, int npts, const float4* __restrict__ sph32,
+                       const double* __restrict__ sph64, double* __restrict__ sasa, int* __restrict__ diag) {
+  extern __shared__ float4 snb[];  // [warps][cap] (rel x, rel y, rel z, thr)
+  int* sidx = (int*)(snb + (blockDim.x >> 5) * cap);
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int i = blockIdx.x * (blockDim.x >> 5) + w, f = blockIdx.y;
+  if (i >= nC) return;
+  float4* nb = snb + w * cap;
+  int* ix = sidx + w * cap;
+  long long o = (long long)f * nC + i;
+  int cnt = min(nbrcnt[o], cap);
+  const int* L = nbr + o * cap;
+  const float4* X = xyz32 + (long long)f * nC;
+  const double* X64 = xyz64 + (long long)f * nC * 3;
+  float4 xi = X[i];
+  bool in_r = i < nR;
+  int split = 0;  // entries with j < nR come first (lists are in slot order)
+  for (int k0 = 0; k0 < cnt; k0 += 32) {
+    int k = k0 + lane;
+    int j = k < cnt ? L[k] : 0;
+    if (k < cnt) {
+      float4 xj = X[j];
+      float ro = (float)(rad64[j] + probe);
+      nb[k] = make_float4(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, ro * ro);
+      ix[k] = j;
+    }
+    split += __popc(__ballot_sync(0xffffffffu, k < cnt && j < nR));
+  }
+  __syncwarp();
+  int own0 = in_r ? 0 : split, own1 = in_r ? split : cnt;
+  int oth0 = in_r ? split : 0, oth1 = in_r ? cnt : split;
+  double er = rad64[i] + probe;
+  float erf = (float)er;
+  int cs = 0, cc = 0, rechecks = 0;
+  for (int p = lane; p < npts; p += 32) {
+    float4 s = sph32[p];
+    float tx = s.x * erf, ty = s.y * erf, tz = s.z * erf;
+    bool bur = false;
+    for (int pass = 0; pass < 2 && !bur; pass++) {
+      int a = pass ? oth0 : own0, b = pass ? oth1 : own1;
+      for (int k = a; k < b; k++) {
+        float4 v = nb[k];
+        float dx = tx - v.x, dy = ty - v.y, dz = tz - v.z;
+        float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (d2 < v.w - kSasaBand) {
+          bur = true;
+          break;
+        }
+        if (d2 <= v.w + kSasaBand) {
+          rechecks++;
+          int j = ix[k];
+          if (exact_buried(X64, i, j, sph64, p, er, __dadd_rn(rad64[j], probe))) {
+            bur = true;
+            break;
+          }
+        }
+      }
+      if (pass == 0 && !bur) cs++;
+    }
+    if (!bur) cc++;
+  }
+  cs = warp_sumi(cs);
+  cc = warp_sumi(cc);
+  rechecks = warp_sumi(rechecks);
+  if (lane == 0) {
+    double area = 4.0 * kPi * (er * er);
+    sasa[2 * o] = ((double)cc / (double)npts) * area;      // in the complex
+    sasa[2 * o + 1] = ((double)cs / (double)npts) * area;  // in its own part
+    if (rechecks) atomicAdd((unsigned long long*)(diag + 6), (unsigned long long)rechecks);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K4: receptor x ligand non-bonded in FP64 (rows per receptor slot, columns
+// per ligand slot)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int pair_class(const int* tile_rec, int nb, const unsigned* masks, int a, int b) {
+  int bi = a / kTile, bj = b / kTile;
+  int rec = tile_rec[bi * nb + bj];
+  if (rec < 0) return 1;
+  int row = a % kTile, col = b % kTile;
+  const unsigned* mr = masks + ((long long)rec * 2 * kTile + row) * 4;
+  if ((mr[kTile * 4 + (col >> 5)] >> (col & 31)) & 1u) return 2;
+  if ((mr[col >> 5] >> (col & 31)) & 1u) return 0;
+  return 1;
+}
+
+__device__ __forceinline__ void rl_pair(const double* X64, const double* q64, const int* type, int nt,
+                                        const double2* lj64, const int* tile_rec, int nb, const unsigned* masks,
+                                        double scee, double scnb, int a, int b, double& v, double& e) {
+  v = 0.0;
+  e = 0.0;
+  int cls = pair_class(tile_rec, nb, masks, a, b);
+  if (!cls) return;
+  double dx = X64[3 * a] - X64[3 * b], dy = X64[3 * a + 1] - X64[3 * b + 1], dz = X64[3 * a + 2] - X64[3 * b + 2];
+  double r2 = dx * dx + dy * dy + dz * dz, r = sqrt(r2);
+  if (r < 1e-10) return;  // decomposition.rs:247-249
+  double r6 = r2 * r2 * r2, r12 = r6 * r6;
+  double2 ab = lj64[type[a] * nt + type[b]];
+  double qq = q64[a] * q64[b];
+  if (cls == 2) {
+    v = (ab.x / r12 - ab.y / r6) / scnb;
+    e = qq / r / scee;
+  } else {
+    v = ab.x / r12 - ab.y / r6;
+    e = qq / r;
+  }
+}
+
+__global__ void k_rl_rows(int nC, int nR, const double* __restrict__ xyz64, const double* __restrict__ q64,
+                          const int* __restrict__ type, int nt, const double2* __restrict__ lj64,
+                          const int* __restrict__ tile_rec, int nb, const unsigned* __restrict__ masks, double scee,
+                          double scnb, double* __restrict__ rows) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x, f = blockIdx.y;
+  if (a >= nR) return;
+  const double* X64 = xyz64 + (long long)f * nC * 3;
+  double sv = 0.0, se = 0.0;
+  for (int b = nR; b < nC; b++) {
+    double v, e;
+    rl_pair(X64, q64, type, nt, lj64, tile_rec, nb, masks, scee, scnb, a, b, v, e);
+    sv += v;
+    se += e;
+  }
+  long long o = (long long)f * nR + a;
+  rows[2 * o] = sv;
+  rows[2 * o + 1] = se;
+}
+
+__global__ void k_rl_cols(int nC, int nR, const double* __restrict__ xyz64, const double* __restrict__ q64,
+                          const int* __restrict__ type, int nt, const double2* __restrict__ lj64,
+                          const int* __restrict__ tile_rec, int nb, const unsigned* __restrict__ masks, double scee,
+                          double scnb, double* __restrict__ cols) {
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31, f = blockIdx.y;
+  int nL = nC - nR;
+  if (w >= nL) return;
+  int b = nR + w;
+  const double* X64 = xyz64 + (long long)f * nC * 3;
+  double sv = 0.0, se = 0.0;
+  for (int a = lane; a < nR; a += 32) {
+    double v, e;
+    rl_pair(X64, q64, type, nt, lj64, tile_rec, nb, masks, scee, scnb, a, b, v, e);
+    sv += v;
+    se += e;
+  }
+  sv = warp_sum(sv);
+  se = warp_sum(se);
+  if (lane == 0) {
+    long long o = (long long)f * nL + w;
+    cols[2 * o] = sv;
+    cols[2 * o + 1] = se;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K6: bonded terms by part (mm_energy.rs:187-212) and 1-4 class corrections
+// term record: kind (0 bond, 1 angle, 2 dihedral, 3 correction), part
+// (0 receptor, 1 ligand, 2 spanning), atoms a b c d; params p0 p1 p2
+// ---------------------------------------------------------------------------
+struct BTerm {
+  int kind, part, a, b, c, d, cls, pad;
+};
+
+__device__ __forceinline__ void cross3d(const double* u, const double* v, double* o) {
+  o[0] = u[1] * v[2] - u[2] * v[1];
+  o[1] = u[2] * v[0] - u[0] * v[2];
+  o[2] = u[0] * v[1] - u[1] * v[0];
+}
+
+__global__ void k_bonded(int nC, int nterms, const BTerm* __restrict__ terms, const double* __restrict__ par,
+                         const double* __restrict__ xyz64, const double* __restrict__ q64, const int* __restrict__ type,
+                         int nt, const double2* __restrict__ lj64, double scee, double scnb,
+                         double* __restrict__ part) {
+  __shared__ double sh[32];
+  int t = blockIdx.x * blockDim.x + threadIdx.x, f = blockIdx.y;
+  const double* x = xyz64 + (long long)f * nC * 3;
+  double e[5] = {0, 0, 0, 0, 0};  // part R, part L, spanning, corr R, corr L
+  if (t < nterms) {
+    BTerm T = terms[t];
+    const double* P = par + 3 * t;
+    double v = 0.0;
+    if (T.kind == 0) {
+      double dx = x[3 * T.a] - x[3 * T.b], dy = x[3 * T.a + 1] - x[3 * T.b + 1], dz = x[3 * T.a + 2] - x[3 * T.b + 2];
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      v = P[0] * (r - P[1]) * (r - P[1]);
+    } else if (T.kind == 1) {
+      double ba[3], bc[3];
+      for (int d = 0; d < 3; d++) {
+        ba[d] = x[3 * T.a + d] - x[3 * T.b + d];
+        bc[d] = x[3 * T.c + d] - x[3 * T.b + d];
+      }
+      double dot = ba[0] * bc[0] + ba[1] * bc[1] + ba[2] * bc[2];
+      double m1 = sqrt(ba[0] * ba[0] + ba[1] * ba[1] + ba[2] * ba[2]), m2 = sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]);
+      double th = acos(fmin(1.0, fmax(-1.0, dot / (m1 * m2))));
+      v = P[0] * (th - P[1]) * (th - P[1]);
+    } else if (T.kind == 2) {
+      double b1[3], b2[3], b3[3], n1[3], n2[3], m1[3], u[3] = {0, 0, 0};
+      for (int d = 0; d < 3; d++) {
+        b1[d] = x[3 * T.b + d] - x[3 * T.a + d];
+        b2[d] = x[3 * T.c + d] - x[3 * T.b + d];
+        b3[d] = x[3 * T.d + d] - x[3 * T.c + d];
+      }
+      cross3d(b1, b2, n1);
+      cross3d(b2, b3, n2);
+      double len = sqrt(b2[0] * b2[0] + b2[1] * b2[1] + b2[2] * b2[2]);
+      if (!(len < 1e-20))
+        for (int d = 0; d < 3; d++) u[d] = b2[d] / len;
+      cross3d(n1, u, m1);
+      double xx = n1[0] * n2[0] + n1[1] * n2[1] + n1[2] * n2[2], yy = m1[0] * n2[0] + m1[1] * n2[1] + m1[2] * n2[2];
+      v = P[0] * (1.0 + cos(P[1] * atan2(-yy, xx) - P[2]));
+    } else {
+      // pair that is 1-4 in the complex but not in its part: part value minus complex value
+      double2 ab = lj64[type[T.a] * nt + type[T.b]];
+      double qq = q64[T.a] * q64[T.b];
+      double ec = nb64(x, T.a, T.b, qq, ab.x, ab.y, 2, scee, scnb);
+      double es = T.cls ? nb64(x, T.a, T.b, qq, ab.x, ab.y, 1, scee, scnb) : 0.0;
+      e[3 + T.part] = es - ec;
+    }
+    if (T.kind < 3) e[T.part] = v;
+  }
+  for (int q = 0; q < 5; q++) {
+    double s = block_sum(e[q], sh);
+    if (threadIdx.x == 0) part[((long long)f * gridDim.x + blockIdx.x) * 5 + q] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K5: per-frame reduction -> FrameEnergy and per-residue terms
+// ---------------------------------------------------------------------------
+__global__ void k_reduce(int nC, int nR, int nb1, int ntiles, int nbp, const double* __restrict__ k1part,
+                         const double* __restrict__ k2part, const double* __restrict__ sasa,
+                         const double* __restrict__ rows, const double* __restrict__ cols,
+                         const double* __restrict__ bpart, const double* __restrict__ R64,
+                         const double* __restrict__ q64, double gamma, double beta, double f0, int nres,
+                         const int* __restrict__ res_ptr, const int* __restrict__ res_slots,
+                         rstg_frame_energy* __restrict__ out, rstg_residue_energy* __restrict__ decomp) {
+  __shared__ double sh[32];
+  __shared__ double tot[24];
+  int f = blockIdx.x;
+  int nL = nC - nR;
+  double v[24];
+  for (int q = 0; q < 24; q++) v[q] = 0.0;
+  for (int b = threadIdx.x; b < nb1; b += blockDim.x)
+    for (int q = 0; q < 4; q++) v[q] += k1part[((long long)f * nb1 + b) * 4 + q];
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+    for (int q = 0; q < 6; q++) v[4 + q] += k2part[((long long)f * ntiles + t) * 6 + q];
+  for (int s = threadIdx.x; s < nC; s += blockDim.x) {
+    const double* S = sasa + ((long long)f * nC + s) * 2;
+    v[10] += S[0];
+    v[s < nR ? 11 : 12] += S[1];
+    v[13] += S[0] - S[1];
+    const double* R = R64 + ((long long)f * nC + s) * 2;
+    double q = q64[s];
+    v[14] += fabs(f0 * q * q / R[0] - f0 * q * q / R[1]);  // decomposition.rs:320-337
+  }
+  for (int a = threadIdx.x; a < nR; a += blockDim.x) v[15] += rows[((long long)f * nR + a) * 2] + rows[((long long)f * nR + a) * 2 + 1];
+  for (int b = threadIdx.x; b < nbp; b += blockDim.x)
+    for (int q = 0; q < 5; q++) v[16 + q] += bpart[((long long)f * nbp + b) * 5 + q];
+  for (int q = 0; q < 21; q++) {
+    double s = block_sum(v[q], sh);
+    if (threadIdx.x == 0) tot[q] = s;
+  }
+  __syncthreads();
+  double selfC = tot[0], selfR = tot[1], selfL = tot[2], dself = tot[3];
+  // pair sums count each unordered pair once; the reference adds 2 x pair (gb_energy.rs:348)
+  double gbC = 2.0 * tot[4], gbR = 2.0 * tot[5], gbL = 2.0 * tot[6], dgb = 2.0 * tot[7], mmR = tot[8], mmL = tot[9];
+  double SC = tot[10], SR = tot[11], SL = tot[12], dS = tot[13], tw = tot[14], eRL = tot[15];
+  double bR = tot[16], bL = tot[17], bX = tot[18], cR = tot[19], cL = tot[20];
+  double d_polar = dself + dgb;
+  if (threadIdx.x == 0) {
+    rstg_frame_energy e;
+    e.receptor.mm = mmR + bR + cR;
+    e.ligand.mm = mmL + bL + cL;
+    e.complex.mm = mmR + mmL + eRL + bR + bL + bX;
+    e.delta_mm = eRL + bX - cR - cL;
+    e.complex.polar = selfC + gbC;
+    e.receptor.polar = selfR + gbR;
+    e.ligand.polar = selfL + gbL;
+    e.delta_polar = d_polar;
+    e.complex.sa = gamma * SC + beta;
+    e.receptor.sa = gamma * SR + beta;
+    e.ligand.sa = gamma * SL + beta;
+    e.delta_sa = gamma * dS - beta;
+    e.delta_total = e.delta_mm + e.delta_polar + e.delta_sa;
+    out[f] = e;
+  }
+  if (!decomp) return;
+  for (int r = threadIdx.x; r < nres; r += blockDim.x) {
+    rstg_residue_energy x{0.0, 0.0, 0.0, 0.0};
+    double w = 0.0;
+    for (int k = res_ptr[r]; k < res_ptr[r + 1]; k++) {
+      int s = res_slots[k];
+      const double* rc = s < nR ? rows + ((long long)f * nR + s) * 2 : cols + ((long long)f * nL + (s - nR)) * 2;
+      x.vdw += 0.5 * rc[0];
+      x.elec += 0.5 * rc[1];
+      const double* R = R64 + ((long long)f * nC + s) * 2;
+      double q = q64[s];
+      w += fabs(f0 * q * q / R[0] - f0 * q * q / R[1]);
+      const double* S = sasa + ((long long)f * nC + s) * 2;
+      x.sa += gamma * (S[0] - S[1]);
+    }
+    x.polar = tw > 1e-20 ? d_polar * (w / tw) : 0.0;
+    decomp[(long long)f * nres + r] = x;
+  }
+}
+
+// ===========================================================================
+// host side
+// ===========================================================================
+static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  auto spread = [](uint64_t v) {
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+  };
+  return spread(x) | spread(y) << 1 | spread(z) << 2;
+}
+
+System::System(Ctx* c, const Topology& t, const std::vector<int64_t>& rres, const std::vector<int64_t>& lres,
+               const rstg_solvation& s, const rstg_sa_params& sp, const rstg_system_opts& o)
+    : ctx(c), solv(s), sa(sp), opts(o), split(Split::make(t, rres, lres)) {
+  n_top = t.n_atoms;
+  nC = split.complex.n_atoms;
+  nR = split.rec_atoms.size();
+  nL = split.lig_atoms.size();
+  n_res_rec = split.rec_res.size();
+  n_res_lig = split.lig_res.size();
+  if (sa.n_sphere_points < 1) throw Error(RSTG_ERR_INVALID, "n_sphere_points must be >= 1");
+  bool fused = opts.mode == RSTG_MODE_FUSED && solv.method == 0;
+  if (fused) {
+    std::vector<uint8_t> seen(nC, 0);
+    for (int64_t a : split.rec_atoms) seen[a] |= 1;
+    for (int64_t a : split.lig_atoms) seen[a] |= 2;
+    for (auto v : seen)
+      if (v == 3) fused = false;  // receptor and ligand share atoms: evaluate parts independently
+  }
+  if (!fused) {
+    opts.mode = RSTG_MODE_PLAIN;
+    plain = std::make_unique<PlainFrameEval>(c, t, rres, lres, solv, sa);
+  }
+  batch = opts.max_batch_frames > 0 ? opts.max_batch_frames : 0;
+}
+
+System::~System() {
+  if (graph) cudaGraphExecDestroy(graph);
+}
+
+int64_t System::footprint(int64_t F) const {
+  if (opts.mode == RSTG_MODE_PLAIN) return nC * 200 + F * 0;
+  int64_t per = n_top * 24 + nC * (24 + 16 + 16 + 8 + 8 + 4 + (int64_t)nbr_cap * 4 + 16) + nR * 16 + nL * 16 +
+                (n_res_rec + n_res_lig) * 32 + 256;
+  int64_t nb = (nC + kTile - 1) / kTile;
+  per += nb * (nb + 1) / 2 * 48 + nb * 32;
+  return per * F + nC * 128;
+}
+
+void System::prepare_fused(const double* x0) {
+  cudaStream_t st = stream();
+  const Topology& C = split.complex;
+  // slot order: receptor atoms then ligand atoms, each along a Morton curve
+  double mn[3] = {1e300, 1e300, 1e300};
+  for (int64_t a = 0; a < nC; a++)
+    for (int d = 0; d < 3; d++) mn[d] = std::min(mn[d], x0[3 * a + d]);
+  auto code = [&](int64_t a) {
+    uint32_t q[3];
+    for (int d = 0; d < 3; d++) {
+      double v = (x0[3 * a + d] - mn[d]) / 2.0;
+      q[d] = (uint32_t)std::min(std::max(v, 0.0), 2097151.0);
+    }
+    return morton3(q[0], q[1], q[2]);
+  };
+  slot_atom.clear();
+  for (int part = 0; part < 2; part++) {
+    std::vector<int64_t> at = part ? split.lig_atoms : split.rec_atoms;
+    std::vector<std::pair<uint64_t, int64_t>> keyed;
+    for (int64_t a : at) keyed.push_back({code(a), a});
+    std::stable_sort(keyed.begin(), keyed.end(),
+                     [](const std::pair<uint64_t, int64_t>& u, const std::pair<uint64_t, int64_t>& v) { return u.first < v.first; });
+    for (auto& k : keyed) slot_atom.push_back(k.second);
+  }
+  std::vector<int32_t> inv(nC, -1);
+  for (int64_t s = 0; s < nC; s++) inv[slot_atom[s]] = (int32_t)s;
+  slot_src.resize(nC);
+  for (int64_t s = 0; s < nC; s++)
+    slot_src[s] = (int32_t)(split.complex_atoms.empty() ? slot_atom[s] : split.complex_atoms[slot_atom[s]]);
+
+  fp = std::make_unique<FusedParams>();
+  FusedParams& F = *fp;
+  auto up = [&](DevBuf& b, const void* src, size_t bytes) {
+    b = DevBuf(bytes ? bytes : 16, st);
+    if (bytes) RSTG_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, st));
+  };
+  const rstg_gb_params& g = solv.gb;
+  std::vector<float4> P(nC);
+  std::vector<double> q(nC), rho(nC), rad(nC), sj(nC);
+  std::vector<int32_t> ty(nC);
+  for (int64_t s = 0; s < nC; s++) {
+    int64_t a = slot_atom[s];
+    q[s] = C.charges_amber[a];
+    rad[s] = C.radii[a];
+    rho[s] = C.radii[a] - g.offset;
+    sj[s] = C.screen[a] * rho[s];
+    ty[s] = (int32_t)C.type_idx[a];
+    P[s] = make_float4((float)q[s], (float)rho[s], (float)sj[s], (float)(C.radii[a] + sa.probe_radius));
+  }
+  up(F.slot_src, slot_src.data(), nC * 4);
+  up(F.P32, P.data(), nC * sizeof(float4));
+  up(F.q64, q.data(), nC * 8);
+  up(F.rho64, rho.data(), nC * 8);
+  up(F.rad64, rad.data(), nC * 8);
+  up(F.sj64, sj.data(), nC * 8);
+  up(F.type, ty.data(), nC * 4);
+  int nt = (int)std::max<int64_t>(C.n_types, 1);
+  F.nt = nt;
+  std::vector<float2> l32(nt * nt, make_float2(0, 0));
+  std::vector<double2> l64(nt * nt, make_double2(0, 0));
+  for (int a = 0; a < C.n_types; a++)
+    for (int b = 0; b < C.n_types; b++) {
+      int64_t idx = C.nb_index[C.n_types * a + b];
+      if (idx >= 1) {
+        l64[a * nt + b] = make_double2(C.lj_a[idx - 1], C.lj_b[idx - 1]);
+        l32[a * nt + b] = make_float2((float)C.lj_a[idx - 1], (float)C.lj_b[idx - 1]);
+      }
+    }
+  up(F.lj32, l32.data(), l32.size() * sizeof(float2));
+  up(F.lj64, l64.data(), l64.size() * sizeof(double2));
+  // tiles and exclusion / 1-4 masks in slot space
+  int nb = (int)((nC + kTile - 1) / kTile);
+  F.nb = nb;
+  PairClasses pc = PairClasses::build(C);
+  std::vector<int> trec(nb * nb, -1);
+  std::vector<unsigned> masks;
+  auto mark = [&](uint64_t key, int which) {
+    int64_t a = (int64_t)(key >> 32), b = (int64_t)(key & 0xffffffffu);
+    int sa_ = inv[a], sb = inv[b];
+    if (sa_ > sb) std::swap(sa_, sb);
+    int bi = sa_ / kTile, bj = sb / kTile;
+    int& r = trec[bi * nb + bj];
+    if (r < 0) {
+      r = (int)(masks.size() / (2 * kTile * 4));
+      masks.resize(masks.size() + 2 * kTile * 4, 0u);
+    }
+    int row = sa_ % kTile, col = sb % kTile;
+    masks[((size_t)r * 2 * kTile + (which ? kTile : 0) + row) * 4 + (col >> 5)] |= 1u << (col & 31);
+  };
+  for (auto k : pc.excl_keys) mark(k, 0);
+  for (auto k : pc.p14_keys) mark(k, 1);
+  std::vector<int4> tiles;
+  for (int bi = 0; bi < nb; bi++)
+    for (int bj = bi; bj < nb; bj++) tiles.push_back(make_int4(bi, bj, trec[bi * nb + bj], 0));
+  F.ntiles = (int)tiles.size();
+  up(F.tiles, tiles.data(), tiles.size() * sizeof(int4));
+  size_t ljsm = (size_t)nt * nt * sizeof(float2);
+  if (ljsm > 160 * 1024) throw Error(RSTG_ERR_INVALID, "too many Lennard-Jones types for the fused kernels");
+  RSTG_CUDA(cudaFuncSetAttribute(k_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ljsm));
+  up(F.tile_rec, trec.data(), trec.size() * 4);
+  up(F.masks, masks.data(), masks.size() * 4);
+  // sphere points (host libm, as the reference)
+  auto sp64 = fibonacci_sphere(sa.n_sphere_points);
+  F.npts = (int)sa.n_sphere_points;
+  std::vector<float4> sp32(F.npts);
+  for (int p = 0; p < F.npts; p++) sp32[p] = make_float4((float)sp64[3 * p], (float)sp64[3 * p + 1], (float)sp64[3 * p + 2], 0.f);
+  up(F.sphere32, sp32.data(), sp32.size() * sizeof(float4));
+  up(F.sphere64, sp64.data(), sp64.size() * 8);
+  F.probe = sa.probe_radius;
+  // residues: receptor residues then ligand residues, as listed
+  std::vector<int32_t> rp{0}, rs;
+  for (int part = 0; part < 2; part++)
+    for (int64_t r : (part ? split.lig_res : split.rec_res)) {
+      std::vector<int32_t> ss;
+      for (int64_t a : C.select({r})) ss.push_back(inv[a]);
+      std::sort(ss.begin(), ss.end());
+      rs.insert(rs.end(), ss.begin(), ss.end());
+      rp.push_back((int32_t)rs.size());
+    }
+  F.nres = (int)(rp.size() - 1);
+  up(F.res_ptr, rp.data(), rp.size() * 4);
+  up(F.res_slots, rs.data(), rs.size() * 4);
+  // bonded terms by part, and 1-4 class corrections
+  std::vector<BTerm> terms;
+  std::vector<double> par;
+  auto part_of = [&](std::initializer_list<int64_t> atoms) {
+    bool allR = true, allL = true;
+    for (int64_t a : atoms) {
+      int s = inv[a];
+      allR &= s < nR;
+      allL &= s >= nR;
+    }
+    return allR ? 0 : (allL ? 1 : 2);
+  };
+  for (size_t b = 0; b < C.bond_i.size(); b++) {
+    terms.push_back({0, part_of({C.bond_i[b], C.bond_j[b]}), inv[C.bond_i[b]], inv[C.bond_j[b]], 0, 0, 0, 0});
+    par.insert(par.end(), {C.bond_k[C.bond_t[b]], C.bond_req[C.bond_t[b]], 0.0});
+  }
+  for (size_t a = 0; a < C.ang_i.size(); a++) {
+    terms.push_back({1, part_of({C.ang_i[a], C.ang_j[a], C.ang_k[a]}), inv[C.ang_i[a]], inv[C.ang_j[a]],
+                     inv[C.ang_k[a]], 0, 0, 0});
+    par.insert(par.end(), {C.angle_k[C.ang_t[a]], C.angle_teq[C.ang_t[a]], 0.0});
+  }
+  for (size_t d = 0; d < C.dih_i.size(); d++) {
+    terms.push_back({2, part_of({C.dih_i[d], C.dih_j[d], C.dih_k[d], C.dih_l[d]}), inv[C.dih_i[d]], inv[C.dih_j[d]],
+                     inv[C.dih_k[d]], inv[C.dih_l[d]], 0, 0});
+    par.insert(par.end(), {C.dih_pk[C.dih_t[d]], C.dih_pn[C.dih_t[d]], C.dih_phase[C.dih_t[d]]});
+  }
+  // pairs that are 1-4 in the complex through a dihedral spanning the parts
+  // but not 1-4 in the part's own topology
+  for (int part = 0; part < 2; part++) {
+    const Topology& sub = part ? split.lig : split.rec;
+    const std::vector<int64_t>& at = part ? split.lig_atoms : split.rec_atoms;
+    PairClasses spc = PairClasses::build(sub);
+    std::vector<int64_t> loc(nC, -1);
+    for (size_t k = 0; k < at.size(); k++) loc[at[k]] = (int64_t)k;
+    for (auto key : pc.p14_keys) {
+      int64_t a = (int64_t)(key >> 32), b = (int64_t)(key & 0xffffffffu);
+      if (loc[a] < 0 || loc[b] < 0) continue;
+      int cs = spc.cls(loc[a], loc[b]);
+      if (cs == 2) continue;
+      terms.push_back({3, part, inv[a], inv[b], 0, 0, cs, 0});
+      par.insert(par.end(), {0.0, 0.0, 0.0});
+    }
+  }
+  F.nterms = (int)terms.size();
+  up(F.bterms, terms.data(), terms.size() * sizeof(BTerm));
+  up(F.bpar, par.data(), par.size() * 8);
+  // GB constants
+  GbConstF& k = F.gb;
+  double s_ = g.salt_concentration;
+  k.kappa = s_ <= 0.0 ? 0.0 : std::sqrt(8.0 * kPi * 332.0522 * 6.022e-4 * s_ / (g.solvent_dielectric * 0.00198688 * g.temperature));
+  k.inv_ein = 1.0 / g.solute_dielectric;
+  k.inv_eout = 1.0 / g.solvent_dielectric;
+  k.diel_ns = -0.5 * (k.inv_ein - k.inv_eout);
+  k.no_salt = k.kappa <= 0.0;
+  k.cut2 = g.cutoff * g.cutoff;
+  k.fk = (float)(kKScale * k.kappa);
+  k.fie = (float)k.inv_ein;
+  k.fio = (float)k.inv_eout;
+  k.fdns = (float)k.diel_ns;
+  k.fcut2 = (float)std::min(k.cut2, 3.0e38);
+  k.model = g.model;
+  k.rgbmax = g.rgbmax;
+  // neighbour capacity from the first frame (x1.5 + 32 margin; re-sized on overflow)
+  {
+    double cell = 0.0;
+    for (int64_t a = 0; a < nC; a++) cell = std::max(cell, C.radii[a] + sa.probe_radius);
+    cell = std::max(2.0 * cell, 1e-3);
+    std::unordered_map<uint64_t, std::vector<int64_t>> grid;
+    auto cid = [&](int64_t a, int dx, int dy, int dz) {
+      int64_t c[3];
+      for (int d = 0; d < 3; d++) c[d] = (int64_t)std::floor((x0[3 * a + d] - mn[d]) / cell);
+      return ((uint64_t)(c[0] + dx + 1) << 42) | ((uint64_t)(c[1] + dy + 1) << 21) | (uint64_t)(c[2] + dz + 1);
+    };
+    for (int64_t a = 0; a < nC; a++) grid[cid(a, 0, 0, 0)].push_back(a);
+    int64_t mx = 0;
+    for (int64_t a = 0; a < nC; a++) {
+      int64_t cnt = 0;
+      double ea = C.radii[a] + sa.probe_radius;
+      for (int dx = -1; dx <= 1; dx++)
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dz = -1; dz <= 1; dz++) {
+            auto it = grid.find(cid(a, dx, dy, dz));
+            if (it == grid.end()) continue;
+            for (int64_t b : it->second) {
+              if (b == a) continue;
+              double e = ea + C.radii[b] + sa.probe_radius, d2 = 0.0;
+              for (int d = 0; d < 3; d++) d2 += (x0[3 * a + d] - x0[3 * b + d]) * (x0[3 * a + d] - x0[3 * b + d]);
+              if (d2 <= e * e) cnt++;
+            }
+          }
+      mx = std::max(mx, cnt);
+    }
+    nbr_cap = (int)std::max<int64_t>(64, ((mx * 3 / 2 + 32) + 31) / 32 * 32);
+  }
+  if (batch <= 0) {
+    // frames per batch: enough CTAs for every SM several times over, within
+    // a device-memory share of about 2 GB for the batch buffers
+    int64_t per = footprint(1);
+    batch = std::max<int64_t>(1, std::min<int64_t>(256, (int64_t)(2.0e9 / std::max<int64_t>(per, 1))));
+  }
+  perm_ready = true;
+}
+
+void System::ensure_buffers(int64_t frames) {
+  if (frames <= buf_frames) return;
+  cudaStream_t st = stream();
+  int64_t B = frames;
+  int nb1 = (int)((nC + kTile - 1) / kTile);
+  int nbp = std::max(1, (fp->nterms + 255) / 256);
+  in_frames = DevBuf(B * n_top * 3 * 8, st);  // room for float64 input
+  xyz64 = DevBuf(B * nC * 24, st);
+  xyz32 = DevBuf(B * nC * 16, st);
+  R64 = DevBuf(B * nC * 16, st);
+  Rf = DevBuf(B * nC * 16, st);
+  nbr = DevBuf(B * nC * (int64_t)nbr_cap * 4, st);
+  nbrcnt = DevBuf(B * nC * 4, st);
+  sasa = DevBuf(B * nC * 16, st);
+  k1part = DevBuf(B * nb1 * 4 * 8, st);
+  k2part = DevBuf(B * (int64_t)fp->ntiles * 6 * 8, st);
+  rows = DevBuf(B * std::max<int64_t>(nR, 1) * 16, st);
+  cols = DevBuf(B * std::max<int64_t>(nL, 1) * 16, st);
+  bpart = DevBuf(B * nbp * 5 * 8, st);
+  res_buf = DevBuf(B * sizeof(rstg_frame_energy), st);
+  dec_buf = DevBuf(B * std::max<int64_t>(fp->nres, 1) * sizeof(rstg_residue_energy), st);
+  diag = DevBuf(64, st);
+  RSTG_CUDA(cudaMemsetAsync(diag.p, 0, 64, st));
+  size_t sm = (size_t)kSasaWarps * nbr_cap * (sizeof(float4) + sizeof(int));
+  if (sm > 200 * 1024) throw Error(RSTG_ERR_INVALID, "SASA neighbour capacity exceeds shared memory");
+  RSTG_CUDA(cudaFuncSetAttribute(k_sasa, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  buf_frames = B;
+  if (graph) {
+    cudaGraphExecDestroy(graph);
+    graph = nullptr;
+  }
+}
+
+void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_energy* d_out,
+                          rstg_residue_energy* d_decomp, Prof* prof) {
+  auto mark = [&](const char* name, double flops, double bytes) {
+    if (!prof) return;
+    prof->names[prof->n] = name;
+    prof->flops[prof->n] = flops;
+    prof->bytes[prof->n] = bytes;
+    prof->n++;
+    RSTG_CUDA(cudaEventRecord(prof->ev[prof->n], stream()));
+  };
+  if (prof) {
+    prof->n = 0;
+    RSTG_CUDA(cudaEventRecord(prof->ev[0], stream()));
+  }
+  const double Fd = (double)F, nCd = (double)nC, nRd = (double)nR, nLd = (double)nL;
+  // algorithmic operation counts per pair: HCT 32, GB 24 (18 without salt), LJ + Coulomb 22
+  const double gbf = fp && fp->gb.no_salt ? 18.0 : 24.0;
+  const double same_pairs = nRd * (nRd - 1) / 2 + nLd * (nLd - 1) / 2;
+  cudaStream_t st = stream();
+  FusedParams& P = *fp;
+  unsigned Fu = (unsigned)F;
+  int nb1 = (int)((nC + kTile - 1) / kTile);
+  int nbp = std::max(1, (P.nterms + 255) / 256);
+  k_prep<<<dim3((unsigned)((nC + 255) / 256), Fu), 256, 0, st>>>((int)nC, (int)n_top, d_frames, f64 ? 1 : 0,
+                                                                 P.slot_src.as<int>(), P.P32.as<float4>(),
+                                                                 xyz64.as<double>(), xyz32.as<float4>());
+  mark("prep", 0.0, Fd * (n_top * 12.0 + nCd * 40.0));
+  k_psi<<<dim3((unsigned)nb1, Fu), kTile, 0, st>>>((int)nC, (int)nR, xyz32.as<float4>(), xyz64.as<double>(),
+                                                   P.P32.as<float4>(), P.rho64.as<double>(), P.sj64.as<double>(),
+                                                   P.rad64.as<double>(), P.q64.as<double>(), P.gb,
+                                                   (float)P.probe, nbr_cap, nbr.as<int>(), nbrcnt.as<int>(),
+                                                   R64.as<double>(), Rf.as<float4>(), k1part.as<double>(),
+                                                   diag.as<int>());
+  mark("psi", Fd * nCd * (nCd - 1) * 32.0, 0.0);
+  size_t ljsm = (size_t)P.nt * P.nt * sizeof(float2);
+  k_pairs<<<dim3((unsigned)P.ntiles, Fu), kTile, ljsm, st>>>(
+      (int)nC, (int)nR, P.tiles.as<int4>(), xyz32.as<float4>(), xyz64.as<double>(), Rf.as<float4>(), P.type.as<int>(),
+      P.nt, P.lj32.as<float2>(), P.lj64.as<double2>(), P.masks.as<unsigned>(), P.gb, split.complex.scee,
+      split.complex.scnb, k2part.as<double>(), diag.as<int>());
+  mark("pairs", Fd * (nCd * (nCd - 1) / 2 * gbf + same_pairs * (gbf + 22.0)), 0.0);
+  size_t sm = (size_t)kSasaWarps * nbr_cap * (sizeof(float4) + sizeof(int));
+  k_sasa<<<dim3((unsigned)((nC + kSasaWarps - 1) / kSasaWarps), Fu), 32 * kSasaWarps, sm, st>>>(
+      (int)nC, (int)nR, nbr_cap, nbr.as<int>(), nbrcnt.as<int>(), xyz32.as<float4>(), xyz64.as<double>(),
+      P.rad64.as<double>(), P.probe, P.npts, P.sphere32.as<float4>(), P.sphere64.as<double>(), sasa.as<double>(),
+      diag.as<int>());
+  mark("sasa", 0.0, 0.0);
+  int nlaunch = 4;
+  if (nR > 0 && nL > 0) {
+    k_rl_rows<<<dim3((unsigned)((nR + 127) / 128), Fu), 128, 0, st>>>(
+        (int)nC, (int)nR, xyz64.as<double>(), P.q64.as<double>(), P.type.as<int>(), P.nt, P.lj64.as<double2>(),
+        P.tile_rec.as<int>(), P.nb, P.masks.as<unsigned>(), split.complex.scee, split.complex.scnb, rows.as<double>());
+    mark("rl_rows", Fd * nRd * nLd * 22.0, 0.0);
+    k_rl_cols<<<dim3((unsigned)((nL + 7) / 8), Fu), 256, 0, st>>>(
+        (int)nC, (int)nR, xyz64.as<double>(), P.q64.as<double>(), P.type.as<int>(), P.nt, P.lj64.as<double2>(),
+        P.tile_rec.as<int>(), P.nb, P.masks.as<unsigned>(), split.complex.scee, split.complex.scnb, cols.as<double>());
+    mark("rl_cols", Fd * nRd * nLd * 22.0, 0.0);
+    nlaunch += 2;
+  } else {
+    RSTG_CUDA(cudaMemsetAsync(rows.p, 0, rows.bytes, st));
+    RSTG_CUDA(cudaMemsetAsync(cols.p, 0, cols.bytes, st));
+  }
+  if (P.nterms > 0) {
+    k_bonded<<<dim3((unsigned)nbp, Fu), 256, 0, st>>>((int)nC, P.nterms, P.bterms.as<BTerm>(), P.bpar.as<double>(),
+                                                      xyz64.as<double>(), P.q64.as<double>(), P.type.as<int>(), P.nt,
+                                                      P.lj64.as<double2>(), split.complex.scee, split.complex.scnb,
+                                                      bpart.as<double>());
+    mark("bonded", 0.0, 0.0);
+    nlaunch++;
+  } else {
+    RSTG_CUDA(cudaMemsetAsync(bpart.p, 0, bpart.bytes, st));
+  }
+  double f0 = -0.5 * (1.0 / solv.gb.solute_dielectric - 1.0 / solv.gb.solvent_dielectric);
+  k_reduce<<<Fu, 256, 0, st>>>((int)nC, (int)nR, nb1, P.ntiles, nbp, k1part.as<double>(), k2part.as<double>(),
+                               sasa.as<double>(), rows.as<double>(), cols.as<double>(), bpart.as<double>(),
+                               R64.as<double>(), P.q64.as<double>(), sa.surface_tension, sa.offset, f0, P.nres,
+                               P.res_ptr.as<int>(), P.res_slots.as<int>(), d_out, d_decomp);
+  mark("reduce", 0.0, 0.0);
+  nlaunch++;
+  launched(ctx, nlaunch);
+  last_stats[0] += nlaunch;
+}
+
+void System::release_buffers() {
+  if (graph) cudaGraphExecDestroy(graph);
+  graph = nullptr;
+  for (DevBuf* b : {&in_frames, &xyz64, &xyz32, &R64, &Rf, &nbr, &nbrcnt, &sasa, &k1part, &k2part, &rows, &cols, &bpart,
+                    &res_buf, &dec_buf, &diag})
+    *b = DevBuf();
+  buf_frames = 0;
+}
+
+void System::profile(const float* d_frames, int64_t F, int32_t* n, char* names, double* ms, double* flops,
+                     double* bytes) {
+  if (opts.mode != RSTG_MODE_FUSED) throw Error(RSTG_ERR_INVALID, "profiling needs a fused-mode system");
+  cudaStream_t st = stream();
+  if (!perm_ready) {
+    std::vector<float> fr(n_top * 3);
+    RSTG_CUDA(cudaMemcpyAsync(fr.data(), d_frames, fr.size() * 4, cudaMemcpyDeviceToHost, st));
+    RSTG_CUDA(cudaStreamSynchronize(st));
+    std::vector<double> x0(nC * 3);
+    for (int64_t a = 0; a < nC; a++) {
+      int64_t t = split.complex_atoms.empty() ? a : split.complex_atoms[a];
+      for (int d = 0; d < 3; d++) x0[3 * a + d] = fr[3 * t + d];
+    }
+    prepare_fused(x0.data());
+  }
+  ensure_buffers(std::min(F, batch));
+  Prof pr;
+  for (auto& e : pr.ev) RSTG_CUDA(cudaEventCreate(&e));
+  std::vector<double> tot(8, 0.0), fl(8, 0.0), by(8, 0.0);
+  int nk = 0;
+  try {
+    for (int64_t f0 = 0; f0 < F; f0 += batch) {
+      int64_t B = std::min(batch, F - f0);
+      RSTG_CUDA(cudaMemcpyAsync(in_frames.p, d_frames + (size_t)f0 * n_top * 3, (size_t)B * n_top * 12,
+                                cudaMemcpyDeviceToDevice, st));
+      launch_batch(in_frames.p, false, B, res_buf.as<rstg_frame_energy>(), dec_buf.as<rstg_residue_energy>(), &pr);
+      RSTG_CUDA(cudaStreamSynchronize(st));
+      nk = pr.n;
+      for (int k = 0; k < pr.n; k++) {
+        float t = 0.f;
+        RSTG_CUDA(cudaEventElapsedTime(&t, pr.ev[k], pr.ev[k + 1]));
+        tot[k] += t;
+        fl[k] += pr.flops[k];
+        by[k] += pr.bytes[k];
+      }
+    }
+  } catch (...) {
+    for (auto& e : pr.ev) cudaEventDestroy(e);
+    throw;
+  }
+  for (auto& e : pr.ev) cudaEventDestroy(e);
+  *n = nk;
+  for (int k = 0; k < nk; k++) {
+    if (names) {
+      memset(names + 32 * k, 0, 32);
+      strncpy(names + 32 * k, pr.names[k], 31);
+    }
+    if (ms) ms[k] = tot[k];
+    if (flops) flops[k] = fl[k];
+    if (bytes) bytes[k] = by[k];
+  }
+}
+
+int System::graph_kernels() const { return 4 + (nR > 0 && nL > 0 ? 2 : 0) + (fp->nterms > 0 ? 1 : 0) + 1; }
+
+void System::run_plain(const void* frames, bool f64, bool host_in, int64_t F, rstg_frame_energy* out, bool host_out,
+                       rstg_residue_energy* decomp) {
+  cudaStream_t st = stream();
+  std::vector<char> hbuf;
+  const char* src = (const char*)frames;
+  size_t esz = f64 ? 8 : 4;
+  if (!host_in) {
+    hbuf.resize(F * n_top * 3 * esz);
+    RSTG_CUDA(cudaMemcpyAsync(hbuf.data(), frames, hbuf.size(), cudaMemcpyDeviceToHost, st));
+    RSTG_CUDA(cudaStreamSynchronize(st));
+    src = hbuf.data();
+  }
+  std::vector<rstg_frame_energy> res(F);
+  int64_t nres = n_res_rec + n_res_lig;
+  std::vector<rstg_residue_energy> dres(decomp ? F * nres : 0);
+  int64_t before = ctx->launches.load();
+  for (int64_t f = 0; f < F; f++) {
+    std::vector<double> xc(nC * 3);
+    for (int64_t a = 0; a < nC; a++) {
+      int64_t t = split.complex_atoms.empty() ? a : split.complex_atoms[a];
+      for (int d = 0; d < 3; d++) {
+        size_t k = ((size_t)f * n_top + t) * 3 + d;
+        xc[3 * a + d] = f64 ? ((const double*)src)[k] : ((double)((const float*)src)[k] * 0.1) * 10.0;
+      }
+    }
+    res[f] = plain->run(xc.data());
+    if (decomp) plain->decompose(xc.data(), solv.gb, &dres[f * nres], &dres[f * nres + n_res_rec]);
+  }
+  last_stats[0] = ctx->launches.load() - before;
+  if (host_out) {
+    memcpy(out, res.data(), F * sizeof(rstg_frame_energy));
+    if (decomp) memcpy(decomp, dres.data(), dres.size() * sizeof(rstg_residue_energy));
+  } else {
+    RSTG_CUDA(cudaMemcpyAsync(out, res.data(), F * sizeof(rstg_frame_energy), cudaMemcpyHostToDevice, st));
+    if (decomp)
+      RSTG_CUDA(cudaMemcpyAsync(decomp, dres.data(), dres.size() * sizeof(rstg_residue_energy), cudaMemcpyHostToDevice, st));
+    RSTG_CUDA(cudaStreamSynchronize(st));
+  }
+}
+
+void System::run(const void* frames, bool f64, bool host_in, int64_t F, rstg_frame_energy* out, bool host_out,
+                 rstg_residue_energy* decomp_out) {
+  if (F <= 0) return;
+  if (opts.mode == RSTG_MODE_PLAIN) {
+    run_plain(frames, f64, host_in, F, out, host_out, decomp_out);
+    return;
+  }
+  cudaStream_t st = stream();
+  size_t esz = f64 ? 8 : 4;
+  if (!perm_ready) {
+    std::vector<double> x0(nC * 3);
+    std::vector<char> fr(n_top * 3 * esz);
+    if (host_in)
+      memcpy(fr.data(), frames, fr.size());
+    else {
+      RSTG_CUDA(cudaMemcpyAsync(fr.data(), frames, fr.size(), cudaMemcpyDeviceToHost, st));
+      RSTG_CUDA(cudaStreamSynchronize(st));
+    }
+    for (int64_t a = 0; a < nC; a++) {
+      int64_t t = split.complex_atoms.empty() ? a : split.complex_atoms[a];
+      for (int d = 0; d < 3; d++)
+        x0[3 * a + d] = f64 ? ((double*)fr.data())[3 * t + d] : (double)((float*)fr.data())[3 * t + d];
+    }
+    prepare_fused(x0.data());
+  }
+  int64_t nres = fp->nres;
+  for (int attempt = 0; attempt < 3; attempt++) {
+    ensure_buffers(std::min(F, batch));
+    RSTG_CUDA(cudaMemsetAsync(diag.p, 0, 64, st));
+    last_stats[0] = 0;
+    for (int64_t f0 = 0; f0 < F; f0 += batch) {
+      int64_t B = std::min(batch, F - f0);
+      const char* src = (const char*)frames + (size_t)f0 * n_top * 3 * esz;
+      RSTG_CUDA(cudaMemcpyAsync(in_frames.p, src, (size_t)B * n_top * 3 * esz,
+                                host_in ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+      bool want_dec = decomp_out != nullptr;
+      rstg_residue_energy* dd = want_dec ? dec_buf.as<rstg_residue_energy>() : nullptr;
+      bool use_graph = opts.use_graphs && B == batch;
+      if (use_graph && (!graph || graph_frames != B || graph_input_f64 != (int)f64 || graph_decomp != (void*)dd)) {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        cudaGraph_t g;
+        RSTG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int64_t before = last_stats[0];
+        try {
+          launch_batch(in_frames.p, f64, B, res_buf.as<rstg_frame_energy>(), dd);
+        } catch (...) {
+          cudaStreamEndCapture(st, &g);
+          throw;
+        }
+        RSTG_CUDA(cudaStreamEndCapture(st, &g));
+        RSTG_CUDA(cudaGraphInstantiate(&graph, g, 0));
+        cudaGraphDestroy(g);
+        graph_frames = B;
+        graph_input_f64 = (int)f64;
+        graph_decomp = dd;
+        last_stats[0] = before;  // the captured launches run below
+        ctx->launches -= graph_kernels();
+      }
+      if (use_graph) {
+        RSTG_CUDA(cudaGraphLaunch(graph, st));
+        ctx->launches += graph_kernels();
+        last_stats[0] += graph_kernels();
+      } else {
+        launch_batch(in_frames.p, f64, B, res_buf.as<rstg_frame_energy>(), dd);
+      }
+      auto kind = host_out ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+      RSTG_CUDA(cudaMemcpyAsync(out + f0, res_buf.p, B * sizeof(rstg_frame_energy), kind, st));
+      if (want_dec)
+        RSTG_CUDA(cudaMemcpyAsync(decomp_out + f0 * nres, dec_buf.p, B * nres * sizeof(rstg_residue_energy), kind, st));
+    }
+    int h[16];
+    RSTG_CUDA(cudaMemcpyAsync(h, diag.p, 64, cudaMemcpyDeviceToHost, st));
+    RSTG_CUDA(cudaStreamSynchronize(st));
+    unsigned long long n64, nre;
+    memcpy(&n64, h + 4, 8);
+    memcpy(&nre, h + 6, 8);
+    last_stats[1] = (int64_t)n64;
+    last_stats[2] = (int64_t)nre;
+    last_stats[3] = h[3];
+    if (h[3] <= nbr_cap) return;
+    // a neighbour list overflowed: grow the capacity and run again
+    nbr_cap = ((h[3] * 3 / 2 + 32) + 31) / 32 * 32;
+    buf_frames = 0;
+  }
+  throw Error(RSTG_ERR_INVALID, "SASA neighbour list capacity could not be sized");
+}
+
+}  // namespace rstg

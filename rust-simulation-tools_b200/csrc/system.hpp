@@ -1,0 +1,86 @@
+// Device-resident batched binding engine (rstg_system).
+#pragma once
+#include <memory>
+
+#include "frame_plain.hpp"
+#include "internal.hpp"
+
+namespace rstg {
+
+constexpr int kTile = 128;  // rows per CTA and columns per shared-memory tile
+
+struct FusedParams;  // system.cu
+
+struct System {
+  Ctx* ctx = nullptr;
+  std::recursive_mutex mu;        // one run at a time per system
+  cudaStream_t stream_ = nullptr;  // fused-mode stream (null: the context's)
+  cudaStream_t stream() const { return stream_ ? stream_ : ctx->stream; }
+  rstg_solvation solv{};
+  rstg_sa_params sa{};
+  rstg_system_opts opts{};
+  Split split;
+  int64_t n_top = 0;  // atoms per input frame (topology atoms)
+  int64_t nC = 0, nR = 0, nL = 0, n_res_rec = 0, n_res_lig = 0;
+
+  // plain mode (and PB): per-frame FP64 evaluation
+  std::unique_ptr<PlainFrameEval> plain;
+
+  // fused mode
+  bool perm_ready = false;
+  std::vector<int64_t> slot_atom;  // slot -> complex atom
+  std::vector<int32_t> slot_src;   // slot -> topology atom (input frame index)
+  std::unique_ptr<FusedParams> fp;
+  int64_t batch = 0;  // frames per device batch
+  int nbr_cap = 320;
+
+  // per-batch buffers (fused)
+  DevBuf in_frames, xyz64, xyz32, R64, Rf, nbr, nbrcnt, sasa, k1part, k2part, rows, cols, bpart, res_buf, dec_buf,
+      diag;
+  int64_t buf_frames = 0;
+  cudaGraphExec_t graph = nullptr;
+  int64_t graph_frames = 0;
+  int graph_input_f64 = -1;
+  const void* graph_src = nullptr;
+  void* graph_out = nullptr;
+  void* graph_decomp = nullptr;
+  int64_t last_stats[4] = {0, 0, 0, 0};
+
+  System(Ctx* c, const Topology& t, const std::vector<int64_t>& rres, const std::vector<int64_t>& lres,
+         const rstg_solvation& s, const rstg_sa_params& sa, const rstg_system_opts& o);
+  ~System();
+  int64_t footprint(int64_t frames) const;
+  void release_buffers();  // frees the per-batch device buffers
+  // frames: [F][n_top][3]; f64 selects float64 Angstrom input (else float32
+  // Angstrom through the DCD nm round trip).  host_* true: host pointers.
+  void run(const void* frames, bool f64, bool host_in, int64_t F, rstg_frame_energy* out, bool host_out,
+           rstg_residue_energy* decomp);
+
+ private:
+  void prepare_fused(const double* first_frame_complex);
+  void ensure_buffers(int64_t frames);
+  // prof (optional): events recorded before the first and after every kernel;
+  // names/flops/bytes receive one entry per kernel.
+  struct Prof {
+    cudaEvent_t ev[9];
+    const char* names[8];
+    double flops[8], bytes[8];
+    int n = 0;
+  };
+  void launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_energy* d_out,
+                    rstg_residue_energy* d_decomp, Prof* prof = nullptr);
+
+ public:
+  void profile(const float* d_frames, int64_t F, int32_t* n, char* names, double* ms, double* flops, double* bytes);
+
+ private:
+  void run_plain(const void* frames, bool f64, bool host_in, int64_t F, rstg_frame_energy* out, bool host_out,
+                 rstg_residue_energy* decomp);
+  int graph_kernels() const;
+};
+
+}  // namespace rstg
+
+struct rstg_system : rstg::System {
+  using rstg::System::System;
+};
