@@ -224,6 +224,22 @@ rstg_status rstg_decompose(rstg_ctx* ctx, const rstg_topology* t, const double* 
                            int64_t n_lig, const rstg_gb_params* gb, const rstg_sa_params* sa,
                            rstg_residue_energy* rec_out, rstg_residue_energy* lig_out);
 
+/* GB energy (Born radii + pair sum, same kernels and results as
+ * rstg_gb_energy_compute) that allocates no device memory.  No counterpart in
+ * the reference.  For callers that cannot call cudaMalloc where they need the
+ * energy (an allocator owned by a host framework, latency-critical loops that
+ * must not enter the driver's allocator).  All pointers are device memory on
+ * the calling thread's current device; d_born_radii may be NULL.  Work is
+ * enqueued on `stream` (NULL: the legacy default stream) and the call returns
+ * without synchronising.  Scratch lives in a 1.5 MiB file-scope device array
+ * that every GPU loading the library holds until exit; n_atoms is limited to
+ * 1..131072 (larger requests fail with RSTG_ERR_INVALID).  The first call on a
+ * device resolves the array's address and should come before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race. */
+rstg_status rstg_gb_energy_noalloc_async(const double* d_xyz, const double* d_charges_amber, const double* d_radii,
+                                         const double* d_screen, int64_t n_atoms, const rstg_gb_params* params,
+                                         double* d_total, double* d_born_radii, void* stream);
+
 /* ---- batched engine ------------------------------------------------------ */
 
 typedef enum rstg_mode {

@@ -178,11 +178,6 @@ void plain_born_radii(Ctx* c, const DevTopo& t, const double* d_xyz, const rstg_
 // GB energy from radii, gb_energy.rs:283-355.  Warp w handles rows w and
 // n-1-w (balanced triangle); per-warp partials are summed in fixed order.
 // ---------------------------------------------------------------------------
-struct GbConst {
-  double kappa, inv_ein, inv_eout, diel_ns, cut2;
-  int no_salt;
-};
-
 __device__ __forceinline__ double gb_pair64(double qi, double qj, double r2, double Ri, double Rj, const GbConst& k) {
   double rr = Ri * Rj;
   double f = sqrt(r2 + rr * exp(-r2 / (4.0 * rr)));

@@ -36,4 +36,19 @@ void plain_decomp_pairs(Ctx* c, const DevTopo& C, const double* d_xyz, const int
 // Deterministic column sums: in [rows][cols] -> out[cols] (fixed order).
 void sum_columns(Ctx* c, const double* d_in, int64_t rows, int cols, double* d_out);
 
+// GB constants of gb_energy.rs:290-306 and the plain kernels behind
+// plain_born_radii / plain_gb_energy / sum_columns (8 warps per block for the
+// first two; part[] holds one partial per warp of (n + 1) / 2 warps).
+struct GbConst {
+  double kappa, inv_ein, inv_eout, diel_ns, cut2;
+  int no_salt;
+};
+GbConst gb_const(const rstg_gb_params& p);
+__global__ void k_born_radii_plain(int n, const double* __restrict__ xyz, const double* __restrict__ rad,
+                                   const double* __restrict__ scr, double offset, double cut2, int model,
+                                   double rgbmax, double* __restrict__ R);
+__global__ void k_gb_plain(int n, const double* __restrict__ xyz, const double* __restrict__ q,
+                           const double* __restrict__ R, GbConst k, double* __restrict__ part);
+__global__ void k_sum_columns(const double* __restrict__ in, long long rows, int cols, double* __restrict__ out);
+
 }  // namespace rstg

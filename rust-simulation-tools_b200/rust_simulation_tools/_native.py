@@ -128,6 +128,7 @@ _sig("rstg_pb_energy_compute", C.c_int, vp, vp, dp, i64, P(PbParams), ip, i64, d
 _sig("rstg_binding_frame", C.c_int, vp, vp, dp, i64, ip, i64, ip, i64, P(Solvation), P(SaParams), P(FrameEnergy))
 _sig("rstg_decompose", C.c_int, vp, vp, dp, i64, ip, i64, ip, i64, P(GbParams), P(SaParams), P(ResidueEnergy),
      P(ResidueEnergy))
+_sig("rstg_gb_energy_noalloc_async", C.c_int, vp, vp, vp, vp, i64, P(GbParams), vp, vp, vp)
 _sig("rstg_system_opts_default", None, P(SystemOpts))
 _sig("rstg_system_create", C.c_int, vp, vp, ip, i64, ip, i64, P(Solvation), P(SaParams), P(SystemOpts), P(vp))
 _sig("rstg_system_destroy", None, vp)
