@@ -212,6 +212,18 @@ rstg_status rstg_sa_energy_compute(rstg_ctx* ctx, const rstg_topology* t, const 
 rstg_status rstg_pb_energy_compute(rstg_ctx* ctx, const rstg_topology* t, const double* xyz, int64_t n,
                                    const rstg_pb_params* p, const int64_t* solute_residues, int64_t n_solute,
                                    double* total, rstg_pb_diag* diag);
+/* Grid set-up of one PB solve (pb_grid.rs:188-985, pb_solver.rs:68-93), for
+ * inspection: auto_grid dims and origin always; when charge != NULL (arrays of
+ * dims[0]*dims[1]*dims[2]) the charge density, SES inside flags (may be NULL),
+ * face dielectrics, kappa-bar^2 map and a grid holding the Debye-Hueckel
+ * boundary potential (zero inside).  eps_out and use_ionic select the
+ * solvated (solvent dielectric, salt) or reference (solute dielectric, none)
+ * solve. */
+rstg_status rstg_pb_grid_maps(rstg_ctx* ctx, const double* xyz, int64_t n, const double* charges_e,
+                              const double* radii, const rstg_pb_params* p, double eps_in, double eps_out,
+                              int32_t use_ionic, int64_t* dims3, double* origin3, double* charge, uint8_t* inside,
+                              double* eps_x, double* eps_y, double* eps_z, double* kappa_sq, double* boundary_phi);
+
 /* compute_binding_energy_single_frame, crates/mmpbsa/src/binding.rs:749-786 */
 rstg_status rstg_binding_frame(rstg_ctx* ctx, const rstg_topology* t, const double* xyz, int64_t n,
                                const int64_t* receptor_residues, int64_t n_rec, const int64_t* ligand_residues,

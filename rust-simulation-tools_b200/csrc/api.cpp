@@ -4,6 +4,7 @@
 #include <memory>
 
 #include "frame_plain.hpp"
+#include "pb.cuh"
 #include "internal.hpp"
 #include "system.hpp"
 #include "trajectory.hpp"
@@ -505,6 +506,31 @@ rstg_status rstg_pb_energy_compute(rstg_ctx* c, const rstg_topology* t, const do
     }
     if (diag) memset(diag, 0, sizeof(*diag));
     *total = top->n_atoms ? pb_energy_run(c, x, top->charges, top->radii, pp, diag) : 0.0;
+  });
+}
+
+rstg_status rstg_pb_grid_maps(rstg_ctx* c, const double* xyz, int64_t n, const double* q, const double* r,
+                              const rstg_pb_params* p, double ein, double eout, int32_t ionic, int64_t* dims,
+                              double* origin, double* charge, uint8_t* inside, double* ex, double* ey, double* ez,
+                              double* k2, double* bphi) {
+  return guard([&] {
+    need(c, "ctx");
+    need(xyz, "xyz");
+    need(q, "charges");
+    need(r, "radii");
+    need(dims, "dims3");
+    need(origin, "origin3");
+    if (n < 1) throw Error(RSTG_ERR_INVALID, "at least one atom is required");
+    if (charge && !(ex && ey && ez && k2 && bphi)) throw Error(RSTG_ERR_INVALID, "all map outputs are required");
+    rstg_pb_params pp;
+    if (p)
+      pp = *p;
+    else
+      rstg_pb_params_default(&pp);
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    c->bind();
+    pb_grid_maps(c, std::vector<double>(xyz, xyz + 3 * n), std::vector<double>(q, q + n), std::vector<double>(r, r + n),
+                 pp, ein, eout, ionic != 0, dims, origin, charge, inside, ex, ey, ez, k2, bphi);
   });
 }
 

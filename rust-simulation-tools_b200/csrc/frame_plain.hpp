@@ -7,10 +7,8 @@
 
 namespace rstg {
 
-struct PbEngine;  // pb.cu
-
-// PB polar energy of one (sub)system (pb_energy.rs:332-438).  xyz_host is
-// Angstrom [n][3]; charges in e.
+// PB polar energy of one (sub)system (pb_energy.rs:332-438), pb.cu.  xyz_host
+// is Angstrom [n][3]; charges in e.
 double pb_energy_run(Ctx* c, const std::vector<double>& xyz_host, const std::vector<double>& q_e,
                      const std::vector<double>& radii, const rstg_pb_params& p, rstg_pb_diag* diag);
 

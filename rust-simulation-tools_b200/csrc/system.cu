@@ -44,6 +44,12 @@ static constexpr float kSasaBand = 2e-4f;  // A^2, FP32 error bound x 10 (see DE
 static constexpr float kNbGuard2 = 3.5f * 3.5f;
 static constexpr int kSasaWarps = 4;
 
+static size_t sasa_smem(int cap) {
+  size_t cap2 = 32;
+  while ((int)cap2 < cap) cap2 <<= 1;
+  return (size_t)kSasaWarps * (cap * sizeof(float4) + cap2 * (sizeof(float) + sizeof(int)));
+}
+
 struct GbConstF {
   double kappa, inv_ein, inv_eout, diel_ns, cut2;
   float fk, fie, fio, fdns, fcut2;
@@ -392,12 +398,17 @@ __global__ void k_sasa(int nC, int nR, int cap, const int* __restrict__ nbr, con
                        const double* __restrict__ rad64, double probe, int npts, const float4* __restrict__ sph32,
                        const double* __restrict__ sph64, double* __restrict__ sasa, int* __restrict__ diag) {
   extern __shared__ float4 snb[];  // [warps][cap] (rel x, rel y, rel z, thr)
-  int* sidx = (int*)(snb + (blockDim.x >> 5) * cap);
+  int nw = blockDim.x >> 5;
+  int cap2 = 32;
+  while (cap2 < cap) cap2 <<= 1;
+  float* skey = (float*)(snb + nw * cap);  // [warps][cap2] sort keys
+  int* sval = (int*)(skey + nw * cap2);    // [warps][cap2] list positions, then atom indices
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int i = blockIdx.x * (blockDim.x >> 5) + w, f = blockIdx.y;
+  int i = blockIdx.x * nw + w, f = blockIdx.y;
   if (i >= nC) return;
   float4* nb = snb + w * cap;
-  int* ix = sidx + w * cap;
+  float* key = skey + w * cap2;
+  int* val = sval + w * cap2;
   long long o = (long long)f * nC + i;
   int cnt = min(nbrcnt[o], cap);
   const int* L = nbr + o * cap;
@@ -405,30 +416,67 @@ __global__ void k_sasa(int nC, int nR, int cap, const int* __restrict__ nbr, con
   const double* X64 = xyz64 + (long long)f * nC * 3;
   float4 xi = X[i];
   bool in_r = i < nR;
-  int split = 0;  // entries with j < nR come first (lists are in slot order)
+  // Order the neighbours: own part first, then the other part, each nearest
+  // first.  Near neighbours bury the largest caps, so buried points (nearly
+  // all of them) exit after a test or two.  Order does not change which
+  // points are accessible.
+  int n_own = 0;
+  for (int k = lane; k < cap2; k += 32) {
+    if (k < cnt) {
+      int j = L[k];
+      float4 xj = X[j];
+      float rx = xj.x - xi.x, ry = xj.y - xi.y, rz = xj.z - xi.z;
+      bool own = (j < nR) == in_r;
+      key[k] = fmaf(rx, rx, fmaf(ry, ry, rz * rz)) + (own ? 0.f : 1.0e6f);
+      val[k] = j;
+    } else {
+      key[k] = 3.0e38f;
+      val[k] = -1;
+    }
+  }
   for (int k0 = 0; k0 < cnt; k0 += 32) {
     int k = k0 + lane;
-    int j = k < cnt ? L[k] : 0;
-    if (k < cnt) {
-      float4 xj = X[j];
-      float ro = (float)(rad64[j] + probe);
-      nb[k] = make_float4(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, ro * ro);
-      ix[k] = j;
-    }
-    split += __popc(__ballot_sync(0xffffffffu, k < cnt && j < nR));
+    bool own = k < cnt && ((L[k] < nR) == in_r);
+    n_own += __popc(__ballot_sync(0xffffffffu, own));
   }
   __syncwarp();
-  int own0 = in_r ? 0 : split, own1 = in_r ? split : cnt;
-  int oth0 = in_r ? split : 0, oth1 = in_r ? cnt : split;
+  for (int size = 2; size <= cap2; size <<= 1)  // bitonic sort of (key, val)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = lane; t < cap2 / 2; t += 32) {
+        int a = 2 * t - (t & (stride - 1)), b = a + stride;
+        bool up = (a & size) == 0;
+        float ka = key[a], kb = key[b];
+        if ((ka > kb) == up) {
+          key[a] = kb;
+          key[b] = ka;
+          int v = val[a];
+          val[a] = val[b];
+          val[b] = v;
+        }
+      }
+      __syncwarp();
+    }
+  for (int k = lane; k < cnt; k += 32) {
+    int j = val[k];
+    float4 xj = X[j];
+    float ro = (float)(rad64[j] + probe);
+    nb[k] = make_float4(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, ro * ro);
+  }
+  __syncwarp();
   double er = rad64[i] + probe;
   float erf = (float)er;
   int cs = 0, cc = 0, rechecks = 0;
-  for (int p = lane; p < npts; p += 32) {
+  // sph32 is stored patch by patch (32 points compact on the sphere per
+  // patch); .w holds the point's index in the reference's order
+  for (int p0 = 0; p0 < npts; p0 += 32) {
+    int p = p0 + lane;
+    if (p >= npts) break;
     float4 s = sph32[p];
+    int pid = __float_as_int(s.w);
     float tx = s.x * erf, ty = s.y * erf, tz = s.z * erf;
     bool bur = false;
     for (int pass = 0; pass < 2 && !bur; pass++) {
-      int a = pass ? oth0 : own0, b = pass ? oth1 : own1;
+      int a = pass ? n_own : 0, b = pass ? cnt : n_own;
       for (int k = a; k < b; k++) {
         float4 v = nb[k];
         float dx = tx - v.x, dy = ty - v.y, dz = tz - v.z;
@@ -439,8 +487,8 @@ __global__ void k_sasa(int nC, int nR, int cap, const int* __restrict__ nbr, con
         }
         if (d2 <= v.w + kSasaBand) {
           rechecks++;
-          int j = ix[k];
-          if (exact_buried(X64, i, j, sph64, p, er, __dadd_rn(rad64[j], probe))) {
+          int j = val[k];
+          if (exact_buried(X64, i, j, sph64, pid, er, __dadd_rn(rad64[j], probe))) {
             bur = true;
             break;
           }
@@ -697,6 +745,37 @@ __global__ void k_reduce(int nC, int nR, int nb1, int ntiles, int nbp, const dou
 // ===========================================================================
 // host side
 // ===========================================================================
+// Order sphere points into patches of 32 that are compact on the sphere
+// (recursive bisection along the axis of largest spread), so one warp's 32
+// points are all buried or all exposed more often than not.
+static void bisect(const std::vector<double>& sp, std::vector<int>& idx, size_t a, size_t b, std::vector<int>& out) {
+  size_t n = b - a;
+  if (n <= 32) {
+    out.insert(out.end(), idx.begin() + a, idx.begin() + b);
+    return;
+  }
+  double lo[3] = {1e9, 1e9, 1e9}, hi[3] = {-1e9, -1e9, -1e9};
+  for (size_t k = a; k < b; k++)
+    for (int d = 0; d < 3; d++) {
+      lo[d] = std::min(lo[d], sp[3 * idx[k] + d]);
+      hi[d] = std::max(hi[d], sp[3 * idx[k] + d]);
+    }
+  int ax = 0;
+  for (int d = 1; d < 3; d++)
+    if (hi[d] - lo[d] > hi[ax] - lo[ax]) ax = d;
+  std::sort(idx.begin() + a, idx.begin() + b, [&](int u, int v) { return sp[3 * u + ax] < sp[3 * v + ax]; });
+  size_t groups = (n + 31) / 32, left = (groups / 2) * 32;
+  bisect(sp, idx, a, a + left, out);
+  bisect(sp, idx, a + left, b, out);
+}
+
+static std::vector<int> sphere_patches(const std::vector<double>& sp, int n) {
+  std::vector<int> idx(n), out;
+  for (int k = 0; k < n; k++) idx[k] = k;
+  bisect(sp, idx, 0, n, out);
+  return out;
+}
+
 static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
   auto spread = [](uint64_t v) {
     v &= 0x1fffff;
@@ -852,8 +931,14 @@ void System::prepare_fused(const double* x0) {
   // sphere points (host libm, as the reference)
   auto sp64 = fibonacci_sphere(sa.n_sphere_points);
   F.npts = (int)sa.n_sphere_points;
+  std::vector<int> order = sphere_patches(sp64, F.npts);
   std::vector<float4> sp32(F.npts);
-  for (int p = 0; p < F.npts; p++) sp32[p] = make_float4((float)sp64[3 * p], (float)sp64[3 * p + 1], (float)sp64[3 * p + 2], 0.f);
+  for (int k = 0; k < F.npts; k++) {
+    int p = order[k];
+    float idx_bits;
+    memcpy(&idx_bits, &p, 4);
+    sp32[k] = make_float4((float)sp64[3 * p], (float)sp64[3 * p + 1], (float)sp64[3 * p + 2], idx_bits);
+  }
   up(F.sphere32, sp32.data(), sp32.size() * sizeof(float4));
   up(F.sphere64, sp64.data(), sp64.size() * 8);
   F.probe = sa.probe_radius;
@@ -996,7 +1081,7 @@ void System::ensure_buffers(int64_t frames) {
   dec_buf = DevBuf(B * std::max<int64_t>(fp->nres, 1) * sizeof(rstg_residue_energy), st);
   diag = DevBuf(64, st);
   RSTG_CUDA(cudaMemsetAsync(diag.p, 0, 64, st));
-  size_t sm = (size_t)kSasaWarps * nbr_cap * (sizeof(float4) + sizeof(int));
+  size_t sm = sasa_smem(nbr_cap);
   if (sm > 200 * 1024) throw Error(RSTG_ERR_INVALID, "SASA neighbour capacity exceeds shared memory");
   RSTG_CUDA(cudaFuncSetAttribute(k_sasa, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   buf_frames = B;
@@ -1046,7 +1131,7 @@ void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_
       P.nt, P.lj32.as<float2>(), P.lj64.as<double2>(), P.masks.as<unsigned>(), P.gb, split.complex.scee,
       split.complex.scnb, k2part.as<double>(), diag.as<int>());
   mark("pairs", Fd * (nCd * (nCd - 1) / 2 * gbf + same_pairs * (gbf + 22.0)), 0.0);
-  size_t sm = (size_t)kSasaWarps * nbr_cap * (sizeof(float4) + sizeof(int));
+  size_t sm = sasa_smem(nbr_cap);
   k_sasa<<<dim3((unsigned)((nC + kSasaWarps - 1) / kSasaWarps), Fu), 32 * kSasaWarps, sm, st>>>(
       (int)nC, (int)nR, nbr_cap, nbr.as<int>(), nbrcnt.as<int>(), xyz32.as<float4>(), xyz64.as<double>(),
       P.rad64.as<double>(), P.probe, P.npts, P.sphere32.as<float4>(), P.sphere64.as<double>(), sasa.as<double>(),

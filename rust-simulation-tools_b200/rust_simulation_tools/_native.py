@@ -125,6 +125,8 @@ _sig("rstg_mm_energy_compute", C.c_int, vp, vp, dp, i64, P(MmEnergy))
 _sig("rstg_gb_energy_compute", C.c_int, vp, vp, dp, i64, P(GbParams), dp, dp)
 _sig("rstg_sa_energy_compute", C.c_int, vp, vp, dp, i64, P(SaParams), dp, dp, dp)
 _sig("rstg_pb_energy_compute", C.c_int, vp, vp, dp, i64, P(PbParams), ip, i64, dp, P(PbDiag))
+_sig("rstg_pb_grid_maps", C.c_int, vp, dp, i64, dp, dp, P(PbParams), dbl, dbl, i32, ip, dp, dp, P(C.c_uint8), dp, dp,
+     dp, dp, dp)
 _sig("rstg_binding_frame", C.c_int, vp, vp, dp, i64, ip, i64, ip, i64, P(Solvation), P(SaParams), P(FrameEnergy))
 _sig("rstg_decompose", C.c_int, vp, vp, dp, i64, ip, i64, ip, i64, P(GbParams), P(SaParams), P(ResidueEnergy),
      P(ResidueEnergy))
