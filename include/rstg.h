@@ -297,6 +297,15 @@ rstg_status rstg_system_run_device(rstg_system* s, const float* d_frames, int64_
  * re-checked in FP64, [3] neighbour-list overflows (must be 0). */
 rstg_status rstg_system_last_stats(const rstg_system* s, int64_t* stats4);
 
+/* Batched Poisson-Boltzmann engine of a fused PB system (no reference
+ * counterpart), accumulated over runs: grids solved, lock-step multigrid
+ * cycles, grids solved by the FP64 path, then host milliseconds of the
+ * set-up (maps, boundary values), the cycles and the finish (fallbacks,
+ * energies).  Eight doubles; zeros for GB systems. */
+rstg_status rstg_system_pb_stats(const rstg_system* s, double* stats8);
+/* Frames per batched PB launch sequence (0: from the device memory budget). */
+rstg_status rstg_system_set_pb_batch(rstg_system* s, int64_t frames);
+
 /* Per-kernel device time of one pass of the fused engine over device frames
  * (no reference counterpart).  Each kernel is bracketed by CUDA events on the
  * system stream (direct launches).  Up to 8 kernels: names [8][32] NUL

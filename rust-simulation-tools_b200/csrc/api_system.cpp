@@ -190,6 +190,29 @@ rstg_status rstg_system_last_stats(const rstg_system* s, int64_t* st) {
   });
 }
 
+rstg_status rstg_system_pb_stats(const rstg_system* s, double* o) {
+  return guard([&] {
+    if (!s || !o) throw Error(RSTG_ERR_INVALID, "system and out must not be NULL");
+    for (int k = 0; k < 8; k++) o[k] = 0.0;
+    if (!s->pbe) return;
+    const rstg::PbBatchStats& t = s->pbe->stats;
+    o[0] = (double)t.jobs;
+    o[1] = (double)t.cycles;
+    o[2] = (double)t.fallbacks;
+    o[3] = t.ms_setup;
+    o[4] = t.ms_cycles;
+    o[5] = t.ms_finish;
+  });
+}
+
+rstg_status rstg_system_set_pb_batch(rstg_system* s, int64_t frames) {
+  return guard([&] {
+    if (!s) throw Error(RSTG_ERR_INVALID, "system must not be NULL");
+    if (frames < 0) throw Error(RSTG_ERR_INVALID, "frames must be >= 0");
+    s->pb_frames_per_batch = frames;
+  });
+}
+
 rstg_status rstg_system_profile(rstg_system* s, const float* d_frames, int64_t F, int32_t* n, char* names,
                                 double* ms, double* flops, double* bytes) {
   return guard([&] {

@@ -135,11 +135,17 @@ PbHash pb_build_hash(const std::vector<double>& x, double max_eff) {
 // result is sparse (8 points per atom) and scattered on the device.
 static void spread_charges(const PbGeom& g, const std::vector<double>& x, const std::vector<double>& q,
                            std::vector<int64_t>& idx, std::vector<double>& val) {
-  std::unordered_map<int64_t, size_t> pos;
   idx.clear();
   val.clear();
   long nx = g.nx, ny = g.ny, nz = g.nz;
   double org[3] = {g.ox, g.oy, g.oz};
+  // open-addressing table: grid index -> position in idx/val (first-touch order)
+  size_t cap = 64;
+  while (cap < 16 * q.size() + 16) cap <<= 1;
+  std::vector<int64_t> key(cap, -1);
+  std::vector<int32_t> pos(cap, 0);
+  idx.reserve(8 * q.size());
+  val.reserve(8 * q.size());
   for (size_t a = 0; a < q.size(); a++) {
     double fc[3];
     for (int d = 0; d < 3; d++) fc[d] = (x[3 * a + d] - org[d]) / g.h;
@@ -154,13 +160,15 @@ static void spread_charges(const PbGeom& g, const std::vector<double>& x, const 
         for (int a2 = 0; a2 < 2; a2++) {
           int64_t k = (ix + a0) + nx * ((iy + a1) + ny * (iz + a2));
           double v = qd * wx[a0] * wy[a1] * wz[a2];
-          auto it = pos.find(k);
-          if (it == pos.end()) {
-            pos.emplace(k, val.size());
+          size_t h = (size_t)((uint64_t)k * 0x9E3779B97F4A7C15ull >> 20) & (cap - 1);
+          while (key[h] != -1 && key[h] != k) h = (h + 1) & (cap - 1);
+          if (key[h] == -1) {  // grid point first touched: 0.0 + v (pb_grid.rs:280-288)
+            key[h] = k;
+            pos[h] = (int32_t)val.size();
             idx.push_back(k);
             val.push_back(0.0 + v);
           } else {
-            val[it->second] += v;
+            val[pos[h]] += v;
           }
         }
   }
@@ -419,23 +427,55 @@ __global__ void k_scatter(const long long* __restrict__ idx, const double* __res
   if (k < m) out[idx[k]] = val[k];
 }
 
-// set_dh_boundary, pb_solver.rs:68-93: atoms summed in order per point.
-// Threads cover every grid point and act on boundary points (pb_solver.rs:31-60
-// visits every point of a grid that is one or two points thick).
-__global__ void k_dh(GeomDev g, const double* __restrict__ xyz, const double* __restrict__ q, int na, double kap,
-                     double eout, double* __restrict__ phi) {
-  __shared__ double sx[256], sy[256], sz[256], sq[256];
-  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long n = (long long)g.nx * g.ny * g.nz;
-  int iz = 0, iy = 0, ix = 0;
-  bool valid = idx < n;
-  if (valid) {
-    iz = (int)(idx / ((long long)g.nx * g.ny));
-    iy = (int)((idx / g.nx) % g.ny);
-    ix = (int)(idx % g.nx);
-    valid = ix == 0 || ix == g.nx - 1 || iy == 0 || iy == g.ny - 1 || iz == 0 || iz == g.nz - 1;
+// Boundary points of a grid enumerated face by face: the two z faces, the
+// two y faces of the interior z planes, the two x faces of the interior
+// rows.  Grids one or two points thick name some points twice (the same
+// value is written twice).
+__device__ __forceinline__ bool boundary_point(const GeomDev& g, long long k, int& ix, int& iy, int& iz) {
+  long long nxy = (long long)g.nx * g.ny;
+  int nzi = max(g.nz - 2, 0), nyi = max(g.ny - 2, 0);
+  if (k < 2 * nxy) {
+    iz = k < nxy ? 0 : g.nz - 1;
+    long long r = k % nxy;
+    ix = (int)(r % g.nx);
+    iy = (int)(r / g.nx);
+    return true;
   }
-  if (!__syncthreads_or(valid)) return;
+  k -= 2 * nxy;
+  long long nyf = (long long)g.nx * nzi;
+  if (k < 2 * nyf) {
+    iy = k < nyf ? 0 : g.ny - 1;
+    long long r = k % nyf;
+    ix = (int)(r % g.nx);
+    iz = 1 + (int)(r / g.nx);
+    return true;
+  }
+  k -= 2 * nyf;
+  long long nxf = (long long)nyi * nzi;
+  if (k < 2 * nxf) {
+    ix = k < nxf ? 0 : g.nx - 1;
+    long long r = k % nxf;
+    iy = 1 + (int)(r % nyi);
+    iz = 1 + (int)(r / nyi);
+    return true;
+  }
+  return false;
+}
+
+static long long boundary_count(const PbGeom& g) {
+  long long nzi = std::max(g.nz - 2, 0), nyi = std::max(g.ny - 2, 0);
+  return 2LL * g.nx * g.ny + 2LL * g.nx * nzi + 2LL * nyi * nzi;
+}
+
+// set_dh_boundary, pb_solver.rs:68-93: atoms summed in order per boundary
+// point (pb_solver.rs:31-60 visits every point of a grid that is one or two
+// points thick; those points are all boundary points).
+__global__ void k_dh(GeomDev g, long long nbnd, const double* __restrict__ xyz, const double* __restrict__ q, int na,
+                     double kap, double eout, double* __restrict__ phi) {
+  __shared__ double sx[256], sy[256], sz[256], sq[256];
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int ix = 0, iy = 0, iz = 0;
+  bool valid = k < nbnd && boundary_point(g, k, ix, iy, iz);
   double p[3];
   grid_point(g, ix, iy, iz, p);
   double s = 0.0;
@@ -451,14 +491,14 @@ __global__ void k_dh(GeomDev g, const double* __restrict__ xyz, const double* __
     __syncthreads();
     int m = min(256, na - a0);
     if (valid)
-      for (int k = 0; k < m; k++) {
-        double dx = p[0] - sx[k], dy = p[1] - sy[k], dz = p[2] - sz[k];
+      for (int j = 0; j < m; j++) {
+        double dx = p[0] - sx[j], dy = p[1] - sy[j], dz = p[2] - sz[j];
         double r = sqrt(dx * dx + dy * dy + dz * dz);
-        if (r > 1e-10) s += conv * sq[k] * exp(-kap * r) / (eout * r);
+        if (r > 1e-10) s += conv * sq[j] * exp(-kap * r) / (eout * r);
       }
     __syncthreads();
   }
-  if (valid) phi[idx] = s;
+  if (valid) phi[ix + (long long)g.nx * (iy + (long long)g.ny * iz)] = s;
 }
 
 // Focusing boundary: fine boundary values interpolated from the coarse
@@ -699,39 +739,27 @@ struct HashBuf {
   }
 };
 
-struct AtomsDev {
-  DevBuf xyz, q, r;
-  int n = 0;
-  std::vector<double> hx, hq, hr;
-  double max_r = 0.0;
-  AtomsDev(const std::vector<double>& x, const std::vector<double>& qe, const std::vector<double>& rad,
-           cudaStream_t st)
-      : hx(x), hq(qe), hr(rad) {
-    n = (int)qe.size();
-    xyz = DevBuf(std::max<size_t>(x.size(), 3) * 8, st);
-    q = DevBuf(std::max<size_t>(qe.size(), 1) * 8, st);
-    r = DevBuf(std::max<size_t>(rad.size(), 1) * 8, st);
-    if (n) {
-      RSTG_CUDA(cudaMemcpyAsync(xyz.p, x.data(), x.size() * 8, cudaMemcpyHostToDevice, st));
-      RSTG_CUDA(cudaMemcpyAsync(q.p, qe.data(), qe.size() * 8, cudaMemcpyHostToDevice, st));
-      RSTG_CUDA(cudaMemcpyAsync(r.p, rad.data(), rad.size() * 8, cudaMemcpyHostToDevice, st));
-    }
-    for (double v : rad) max_r = std::max(max_r, v);
-  }
-};
-
 static unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// Device maps of one grid; MapsView is the non-owning form the solver reads.
+struct MapsView {
+  PbGeom g;
+  const double *rho, *ex, *ey, *ez, *k2;
+};
 
 struct Maps {
   PbGeom g;
   DevBuf rho, ex, ey, ez, k2;
+  MapsView view() const {
+    return MapsView{g, rho.as<double>(), ex.as<double>(), ey.as<double>(), ez.as<double>(), k2.as<double>()};
+  }
 };
 
-// Charge map of a grid (sparse host spreading, device scatter).
-static void charge_map(Ctx* c, const PbGeom& g, const AtomsDev& A, DevBuf& rho) {
-  cudaStream_t st = c->stream;
-  rho = DevBuf(g.n() * 8, st);
-  RSTG_CUDA(cudaMemsetAsync(rho.p, 0, g.n() * 8, st));
+// Charge map of a grid (sparse host spreading, device scatter) into a
+// caller-owned array of g.n() doubles.
+static void charge_into(Ctx* c, const PbGeom& g, const AtomsDev& A, double* rho) {
+  cudaStream_t st = pb_stream(c);
+  RSTG_CUDA(cudaMemsetAsync(rho, 0, g.n() * 8, st));
   std::vector<int64_t> idx;
   std::vector<double> val;
   spread_charges(g, A.hx, A.hq, idx, val);
@@ -740,22 +768,24 @@ static void charge_map(Ctx* c, const PbGeom& g, const AtomsDev& A, DevBuf& rho) 
   RSTG_CUDA(cudaMemcpyAsync(di.p, idx.data(), idx.size() * 8, cudaMemcpyHostToDevice, st));
   RSTG_CUDA(cudaMemcpyAsync(dv.p, val.data(), val.size() * 8, cudaMemcpyHostToDevice, st));
   k_scatter<<<nblk((long long)idx.size(), 256), 256, 0, st>>>(di.as<long long>(), dv.as<double>(), (int)idx.size(),
-                                                              rho.as<double>());
+                                                              rho);
   launched(c);
   RSTG_CUDA(cudaStreamSynchronize(st));  // the host vectors above go out of scope
 }
 
+static void charge_map(Ctx* c, const PbGeom& g, const AtomsDev& A, DevBuf& rho) {
+  rho = DevBuf(g.n() * 8, pb_stream(c));
+  charge_into(c, g, A, rho.as<double>());
+}
+
 // assign_dielectrics (pb_grid.rs:827-940) and assign_kappa (pb_grid.rs:951-985)
-static void dielectric_maps(Ctx* c, Maps& M, const AtomsDev& A, double probe, double ein, double eout) {
-  cudaStream_t st = c->stream;
-  const PbGeom& g = M.g;
+static void dielectric_into(Ctx* c, const PbGeom& g, const AtomsDev& A, double probe, double ein, double eout,
+                            double* ex, double* ey, double* ez) {
+  cudaStream_t st = pb_stream(c);
   long long n = (long long)g.n();
-  M.ex = DevBuf(n * 8, st);
-  M.ey = DevBuf(n * 8, st);
-  M.ez = DevBuf(n * 8, st);
   GeomDev gd = gdev(g);
   if (std::fabs(ein - eout) < std::numeric_limits<double>::epsilon()) {
-    for (DevBuf* b : {&M.ex, &M.ey, &M.ez}) k_fill<<<nblk(n, 256), 256, 0, st>>>(b->as<double>(), n, ein);
+    for (double* b : {ex, ey, ez}) k_fill<<<nblk(n, 256), 256, 0, st>>>(b, n, ein);
     launched(c, 3);
     return;
   }
@@ -801,7 +831,7 @@ static void dielectric_maps(Ctx* c, Maps& M, const AtomsDev& A, double probe, do
   DevBuf ovf(8, st);
   RSTG_CUDA(cudaMemsetAsync(ovf.p, 0, 4, st));
   k_eps<<<nblk(n, 128), 128, 0, st>>>(gd, inside.as<uint8_t>(), he.d, A.xyz.as<double>(), A.r.as<double>(), ein, eout,
-                                      M.ex.as<double>(), M.ey.as<double>(), M.ez.as<double>(), ovf.as<int>());
+                                      ex, ey, ez, ovf.as<int>());
   launched(c);
   int h = 0;
   RSTG_CUDA(cudaMemcpyAsync(&h, ovf.p, 4, cudaMemcpyDeviceToHost, st));
@@ -809,20 +839,33 @@ static void dielectric_maps(Ctx* c, Maps& M, const AtomsDev& A, double probe, do
   if (h) throw Error(RSTG_ERR_INVALID, "more than 64 atom chords on one grid edge");
 }
 
-static void kappa_map(Ctx* c, Maps& M, const AtomsDev& A, double ion, double kap, double eps_s, bool ionic) {
-  cudaStream_t st = c->stream;
+static void dielectric_maps(Ctx* c, Maps& M, const AtomsDev& A, double probe, double ein, double eout) {
+  cudaStream_t st = pb_stream(c);
   long long n = (long long)M.g.n();
-  M.k2 = DevBuf(n * 8, st);
+  M.ex = DevBuf(n * 8, st);
+  M.ey = DevBuf(n * 8, st);
+  M.ez = DevBuf(n * 8, st);
+  dielectric_into(c, M.g, A, probe, ein, eout, M.ex.as<double>(), M.ey.as<double>(), M.ez.as<double>());
+}
+
+static void kappa_into(Ctx* c, const PbGeom& g, const AtomsDev& A, double ion, double kap, double eps_s, bool ionic,
+                       double* k2) {
+  cudaStream_t st = pb_stream(c);
+  long long n = (long long)g.n();
   if (!ionic) {
-    RSTG_CUDA(cudaMemsetAsync(M.k2.p, 0, n * 8, st));
+    RSTG_CUDA(cudaMemsetAsync(k2, 0, n * 8, st));
     return;
   }
   double kbs = eps_s * kap * kap;
   HashBuf hk(pb_build_hash(A.hx, A.max_r + ion), st);
-  k_kappa<<<nblk(n, 256), 256, 0, st>>>(gdev(M.g), hk.d, A.xyz.as<double>(), A.r.as<double>(), ion, kbs,
-                                        M.k2.as<double>());
+  k_kappa<<<nblk(n, 256), 256, 0, st>>>(gdev(g), hk.d, A.xyz.as<double>(), A.r.as<double>(), ion, kbs, k2);
   launched(c);
   RSTG_CUDA(cudaStreamSynchronize(st));
+}
+
+static void kappa_map(Ctx* c, Maps& M, const AtomsDev& A, double ion, double kap, double eps_s, bool ionic) {
+  M.k2 = DevBuf(M.g.n() * 8, pb_stream(c));
+  kappa_into(c, M.g, A, ion, kap, eps_s, ionic, M.k2.as<double>());
 }
 
 struct MgLevel {
@@ -846,10 +889,10 @@ static LevelDev ldev(const PbGeom& g, const double* ex, const double* ey, const 
 struct Solver {
   Ctx* c;
   cudaStream_t st;
-  const Maps& M;
+  MapsView M;
   std::vector<MgLevel> L;
   DevBuf part, scal;
-  Solver(Ctx* cc, const Maps& m) : c(cc), st(cc->stream), M(m) {
+  Solver(Ctx* cc, const MapsView& m) : c(cc), st(pb_stream(cc)), M(m) {
     size_t parts = (size_t)nblk(m.g.nx, 128) * std::max(m.g.ny - 2, 1) * std::max(m.g.nz - 2, 1);
     part = DevBuf(std::max<size_t>(parts, 1) * 8, st);
     scal = DevBuf(64, st);
@@ -857,7 +900,7 @@ struct Solver {
 
   void build_levels() {  // pb_solver.rs:776-836
     PbGeom g = M.g;
-    const double *ex = M.ex.as<double>(), *ey = M.ey.as<double>(), *ez = M.ez.as<double>(), *k2 = M.k2.as<double>();
+    const double *ex = M.ex, *ey = M.ey, *ez = M.ez, *k2 = M.k2;
     for (;;) {
       if (std::min(g.nx, std::min(g.ny, g.nz)) <= 5) break;
       MgLevel lv;
@@ -960,18 +1003,13 @@ struct Solver {
   }
 };
 
-struct BcSpec {
-  int kind = 1;  // 1 Debye-Hueckel, 2 interpolated from a coarse potential
-  double kappa = 0.0, eout = 1.0;
-  const PbGeom* cg = nullptr;
-  const double* cphi = nullptr;
-};
-
 static void apply_bc(Ctx* c, const PbGeom& g, double* phi, const AtomsDev& A, const BcSpec& bc) {
-  cudaStream_t st = c->stream;
+  cudaStream_t st = pb_stream(c);
   long long n = (long long)g.n();
   if (bc.kind == 1) {
-    k_dh<<<nblk(n, 256), 256, 0, st>>>(gdev(g), A.xyz.as<double>(), A.q.as<double>(), A.n, bc.kappa, bc.eout, phi);
+    long long nbnd = boundary_count(g);
+    k_dh<<<nblk(nbnd, 256), 256, 0, st>>>(gdev(g), nbnd, A.xyz.as<double>(), A.q.as<double>(), A.n, bc.kappa, bc.eout,
+                                          phi);
   } else {
     k_interp_boundary<<<nblk(n, 256), 256, 0, st>>>(gdev(g), gdev(*bc.cg), bc.cphi, phi);
   }
@@ -980,8 +1018,8 @@ static void apply_bc(Ctx* c, const PbGeom& g, double* phi, const AtomsDev& A, co
 
 // solve_lpbe_multigrid (pb_solver.rs:1015-1167) with the plain SOR fallback
 // (pb_solver.rs:373-447)
-static SolveOut solve_mg(Ctx* c, const Maps& M, const AtomsDev& A, const BcSpec& bc, double tol, int64_t maxit) {
-  cudaStream_t st = c->stream;
+static SolveOut solve_mg(Ctx* c, const MapsView& M, const AtomsDev& A, const BcSpec& bc, double tol, int64_t maxit) {
+  cudaStream_t st = pb_stream(c);
   const PbGeom& g = M.g;
   long long n = (long long)g.n();
   SolveOut R;
@@ -989,7 +1027,7 @@ static SolveOut solve_mg(Ctx* c, const Maps& M, const AtomsDev& A, const BcSpec&
   RSTG_CUDA(cudaMemsetAsync(R.phi.p, 0, n * 8, st));
   apply_bc(c, g, R.phi.as<double>(), A, bc);
   Solver S(c, M);
-  LevelDev top = ldev(g, M.ex.as<double>(), M.ey.as<double>(), M.ez.as<double>(), M.k2.as<double>());
+  LevelDev top = ldev(g, M.ex, M.ey, M.ez, M.k2);
   auto sor = [&](bool restart) {
     if (restart) RSTG_CUDA(cudaMemsetAsync(R.phi.p, 0, n * 8, st));
     apply_bc(c, g, R.phi.as<double>(), A, bc);
@@ -998,7 +1036,7 @@ static SolveOut solve_mg(Ctx* c, const Maps& M, const AtomsDev& A, const BcSpec&
     R.converged = false;
     for (int64_t it = 0; it < maxit; it++) {
       double rms = 0.0;
-      S.smooth(top, R.phi.as<double>(), M.rho.as<double>(), om, 1, kFourPiEc, &rms);
+      S.smooth(top, R.phi.as<double>(), M.rho, om, 1, kFourPiEc, &rms);
       R.residual = rms;
       R.iterations = it + 1;
       om = it == 0 ? 1.0 / (1.0 - rs2 / 2.0) : 1.0 / (1.0 - rs2 * om / 4.0);
@@ -1019,8 +1057,8 @@ static SolveOut solve_mg(Ctx* c, const Maps& M, const AtomsDev& A, const BcSpec&
   double best = std::numeric_limits<double>::max(), prev = std::numeric_limits<double>::max();
   int growing = 0;
   for (int64_t cyc = 0; cyc < maxv; cyc++) {
-    S.v_cycle(0, g, top, R.phi.as<double>(), M.rho.as<double>(), omega, kFourPiEc);
-    double r = S.rms_residual(top, R.phi.as<double>(), M.rho.as<double>(), kFourPiEc);
+    S.v_cycle(0, g, top, R.phi.as<double>(), M.rho, omega, kFourPiEc);
+    double r = S.rms_residual(top, R.phi.as<double>(), M.rho, kFourPiEc);
     if (r < best) {
       best = r;
       growing = 0;
@@ -1040,14 +1078,14 @@ static SolveOut solve_mg(Ctx* c, const Maps& M, const AtomsDev& A, const BcSpec&
       return R;
     }
   }
-  R.residual = S.rms_residual(top, R.phi.as<double>(), M.rho.as<double>(), kFourPiEc);
+  R.residual = S.rms_residual(top, R.phi.as<double>(), M.rho, kFourPiEc);
   R.iterations = maxv;
   R.converged = false;
   return R;
 }
 
 static double elec_energy(Ctx* c, const PbGeom& g, const double* phi, const AtomsDev& A) {
-  cudaStream_t st = c->stream;
+  cudaStream_t st = pb_stream(c);
   if (A.n == 0) return 0.0;
   DevBuf v(A.n * 8, st), e(8, st);
   k_atom_phi<<<nblk(A.n, 128), 128, 0, st>>>(gdev(g), phi, A.xyz.as<double>(), A.q.as<double>(), A.n, v.as<double>());
@@ -1060,12 +1098,12 @@ static double elec_energy(Ctx* c, const PbGeom& g, const double* phi, const Atom
 }
 
 static double maxabs(Ctx* c, const DevBuf& phi, long long n) {
-  DevBuf o(8, c->stream);
-  k_maxabs<<<1, 1024, 0, c->stream>>>(phi.as<double>(), n, o.as<double>());
+  DevBuf o(8, pb_stream(c));
+  k_maxabs<<<1, 1024, 0, pb_stream(c)>>>(phi.as<double>(), n, o.as<double>());
   launched(c);
   double h = 0.0;
-  RSTG_CUDA(cudaMemcpyAsync(&h, o.p, 8, cudaMemcpyDeviceToHost, c->stream));
-  RSTG_CUDA(cudaStreamSynchronize(c->stream));
+  RSTG_CUDA(cudaMemcpyAsync(&h, o.p, 8, cudaMemcpyDeviceToHost, pb_stream(c)));
+  RSTG_CUDA(cudaStreamSynchronize(pb_stream(c)));
   return h;
 }
 
@@ -1090,28 +1128,28 @@ static double solve_focus(Ctx* c, const Maps& fine_rho, const PbGeom* cg, const 
     charge_map(c, *cg, A, C.rho);
     dielectric_maps(c, C, A, p.probe_radius, ein, eout);
     kappa_map(c, C, A, p.ion_radius, kap, p.solvent_dielectric, ionic);
-    SolveOut cr = solve_mg(c, C, A, dh, p.tolerance * 10.0, p.max_iterations);
+    SolveOut cr = solve_mg(c, C.view(), A, dh, p.tolerance * 10.0, p.max_iterations);
     double mp = maxabs(c, cr.phi, (long long)cg->n());
     bool ok = cr.converged && std::isfinite(mp) && mp < 1e10;
     fine_maps(F);
-    F.rho = DevBuf(fine_rho.g.n() * 8, c->stream);
-    RSTG_CUDA(cudaMemcpyAsync(F.rho.p, fine_rho.rho.p, fine_rho.g.n() * 8, cudaMemcpyDeviceToDevice, c->stream));
+    F.rho = DevBuf(fine_rho.g.n() * 8, pb_stream(c));
+    RSTG_CUDA(cudaMemcpyAsync(F.rho.p, fine_rho.rho.p, fine_rho.g.n() * 8, cudaMemcpyDeviceToDevice, pb_stream(c)));
     if (!ok) {
-      *out = solve_mg(c, F, A, dh, p.tolerance, p.max_iterations);
+      *out = solve_mg(c, F.view(), A, dh, p.tolerance, p.max_iterations);
     } else {
       BcSpec ib;
       ib.kind = 2;
       ib.cg = cg;
       ib.cphi = cr.phi.as<double>();
-      *out = solve_mg(c, F, A, ib, p.tolerance, p.max_iterations);
-      RSTG_CUDA(cudaStreamSynchronize(c->stream));
+      *out = solve_mg(c, F.view(), A, ib, p.tolerance, p.max_iterations);
+      RSTG_CUDA(cudaStreamSynchronize(pb_stream(c)));
     }
     return elec_energy(c, F.g, out->phi.as<double>(), A);
   }
   fine_maps(F);
-  F.rho = DevBuf(fine_rho.g.n() * 8, c->stream);
-  RSTG_CUDA(cudaMemcpyAsync(F.rho.p, fine_rho.rho.p, fine_rho.g.n() * 8, cudaMemcpyDeviceToDevice, c->stream));
-  *out = solve_mg(c, F, A, dh, p.tolerance, p.max_iterations);
+  F.rho = DevBuf(fine_rho.g.n() * 8, pb_stream(c));
+  RSTG_CUDA(cudaMemcpyAsync(F.rho.p, fine_rho.rho.p, fine_rho.g.n() * 8, cudaMemcpyDeviceToDevice, pb_stream(c)));
+  *out = solve_mg(c, F.view(), A, dh, p.tolerance, p.max_iterations);
   return elec_energy(c, F.g, out->phi.as<double>(), A);
 }
 
@@ -1129,7 +1167,7 @@ void pb_grid_maps(Ctx* c, const std::vector<double>& x, const std::vector<double
   origin[1] = g.oy;
   origin[2] = g.oz;
   if (!charge) return;
-  cudaStream_t st = c->stream;
+  cudaStream_t st = pb_stream(c);
   AtomsDev A(x, q, radii, st);
   Maps M;
   M.g = g;
@@ -1199,7 +1237,7 @@ double pb_energy_run(Ctx* c, const std::vector<double>& x, const std::vector<dou
   double s = p.salt_concentration;
   double kap = s <= 0.0 ? 0.0
                         : std::sqrt(8.0 * kPi * 332.0522 * 6.022e-4 * s / (p.solvent_dielectric * 0.00198688 * p.temperature));
-  AtomsDev A(x, q, radii, c->stream);
+  AtomsDev A(x, q, radii, pb_stream(c));
   Maps fine;
   fine.g = pb_auto_grid(x, p.grid_spacing, p.grid_buffer);
   if (fine.g.n() > (size_t)600 * 600 * 600) throw Error(RSTG_ERR_NOMEM, "PB grid exceeds 600^3 points");
@@ -1222,6 +1260,55 @@ double pb_energy_run(Ctx* c, const std::vector<double>& x, const std::vector<dou
     diag->dims[2] = fine.g.nz;
   }
   return es - er;
+}
+
+// ---------------------------------------------------------------------------
+// entry points of the batched engine (pb_batch.cu)
+// ---------------------------------------------------------------------------
+static thread_local cudaStream_t t_pb_stream = nullptr;
+cudaStream_t pb_stream(Ctx* c) { return t_pb_stream ? t_pb_stream : c->stream; }
+PbStreamScope::PbStreamScope(cudaStream_t s) : prev(t_pb_stream) { t_pb_stream = s; }
+PbStreamScope::~PbStreamScope() { t_pb_stream = prev; }
+
+double pb_kappa(const rstg_pb_params& p) {  // pb_energy.rs:337-345
+  double s = p.salt_concentration;
+  return s <= 0.0 ? 0.0
+                  : std::sqrt(8.0 * kPi * 332.0522 * 6.022e-4 * s / (p.solvent_dielectric * 0.00198688 * p.temperature));
+}
+
+void pb_maps_into(Ctx* c, const PbGeom& g, const AtomsDev& A, const rstg_pb_params& p, double ein, double eout,
+                  double kap, bool ionic, double* rho, double* ex, double* ey, double* ez, double* k2) {
+  if (rho) charge_into(c, g, A, rho);
+  if (ex) dielectric_into(c, g, A, p.probe_radius, ein, eout, ex, ey, ez);
+  if (k2) kappa_into(c, g, A, p.ion_radius, kap, p.solvent_dielectric, ionic, k2);
+}
+
+void pb_boundary(Ctx* c, const PbGeom& g, double* phi, const AtomsDev& A, const BcSpec& bc) { apply_bc(c, g, phi, A, bc); }
+
+PbSolveStats pb_solve_fp64(Ctx* c, const PbGeom& g, const double* rho, const double* ex, const double* ey,
+                           const double* ez, const double* k2, double uniform_eps, const AtomsDev& A,
+                           const BcSpec& bc, double tol, int64_t maxit, double* phi_out) {
+  cudaStream_t st = pb_stream(c);
+  long long n = (long long)g.n();
+  DevBuf fx, fy, fz, fk;
+  if (!ex) {
+    fx = DevBuf(n * 8, st);
+    fy = DevBuf(n * 8, st);
+    fz = DevBuf(n * 8, st);
+    fk = DevBuf(n * 8, st);
+    for (DevBuf* b : {&fx, &fy, &fz}) k_fill<<<nblk(n, 256), 256, 0, st>>>(b->as<double>(), n, uniform_eps);
+    RSTG_CUDA(cudaMemsetAsync(fk.p, 0, n * 8, st));
+    launched(c, 3);
+    ex = fx.as<double>();
+    ey = fy.as<double>();
+    ez = fz.as<double>();
+    k2 = fk.as<double>();
+  }
+  MapsView M{g, rho, ex, ey, ez, k2};
+  SolveOut R = solve_mg(c, M, A, bc, tol, maxit);
+  RSTG_CUDA(cudaMemcpyAsync(phi_out, R.phi.p, n * 8, cudaMemcpyDeviceToDevice, st));
+  RSTG_CUDA(cudaStreamSynchronize(st));
+  return PbSolveStats{R.iterations, R.residual, R.converged};
 }
 
 }  // namespace rstg

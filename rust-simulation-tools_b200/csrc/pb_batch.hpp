@@ -1,0 +1,63 @@
+// Batched mixed-precision Poisson-Boltzmann engine (pb_batch.cu).
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "pb.cuh"
+
+namespace rstg {
+
+// One grid solve of a batch.
+struct PbJob {
+  PbGeom g;
+  const AtomsDev* atoms = nullptr;
+  bool uniform = false;  // reference solve: dielectric ein everywhere, kbar^2 = 0
+  bool ionic = false;    // kbar^2 map from the ion-accessible region
+  double ein = 1.0, eout = 80.0, kap = 0.0;
+  BcSpec bc;             // Debye-Hueckel, or interpolated from bc.cphi on *bc.cg
+  double tol = 1e-6;
+  int64_t maxit = 10000;
+  bool energy = true;    // 0.5 sum q phi(atom) wanted
+  // results
+  PbSolveStats stats{};
+  double e = 0.0;        // energy (kcal/mol) when requested
+  double maxabs = 0.0;   // max |phi| over the grid
+  bool fallback = false; // solved by the FP64 path (grid too small for multigrid, or divergence)
+};
+
+struct PbBatchStats {
+  int64_t cycles = 0;      // lock-step cycles run
+  int64_t fallbacks = 0;   // jobs solved by the FP64 path
+  int64_t jobs = 0;
+  double ms_setup = 0.0;   // maps and boundary values
+  double ms_cycles = 0.0;  // lock-step multigrid cycles
+  double ms_finish = 0.0;  // FP64 fallbacks, energies
+};
+
+class PbBatchEngine {
+ public:
+  PbBatchEngine(Ctx* c, cudaStream_t st) : c_(c), st_(st) {}
+  ~PbBatchEngine();
+  // Builds maps and boundary values of every job, solves them in lock step
+  // and fills stats / e / maxabs.  keep_phi: copy each job's potential into
+  // phi_out[j] (device arrays of g.n() doubles, may be null per job).
+  void solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, const std::vector<double*>* phi_out = nullptr);
+  void set_stream(cudaStream_t s) { st_ = s; }
+  PbBatchStats stats;
+  int chunk_cycles = 8;  // cycles per graph launch between status reads
+
+ private:
+  Ctx* c_;
+  cudaStream_t st_;
+  DevBuf pool64_, pool32_, desc_, part_, small_, lists_;
+  cudaGraphExec_t graph_ = nullptr;
+};
+
+// Polar PB energies (E_solvated - E_reference, pb_energy.rs:332-438) of
+// n_sets atom sets, batched.  xyz[i]: host Angstrom coordinates; q in e.
+// out[i] receives the energy, diag[i] (optional) the solve statistics.
+void pb_polar_batch(Ctx* c, cudaStream_t st, PbBatchEngine& eng, const rstg_pb_params& p,
+                    const std::vector<const std::vector<double>*>& xyz, const std::vector<const std::vector<double>*>& q,
+                    const std::vector<const std::vector<double>*>& r, double* out, rstg_pb_diag* diag);
+
+}  // namespace rstg

@@ -799,7 +799,8 @@ System::System(Ctx* c, const Topology& t, const std::vector<int64_t>& rres, cons
   n_res_rec = split.rec_res.size();
   n_res_lig = split.lig_res.size();
   if (sa.n_sphere_points < 1) throw Error(RSTG_ERR_INVALID, "n_sphere_points must be >= 1");
-  bool fused = opts.mode == RSTG_MODE_FUSED && solv.method == 0;
+  bool fused = opts.mode == RSTG_MODE_FUSED && (solv.method == 0 || solv.method == 1);
+  if (solv.method == 1) rstg_gb_params_default(&solv.gb);  // GB kernels run with defaults; PB gives the polar terms
   if (fused) {
     std::vector<uint8_t> seen(nC, 0);
     for (int64_t a : split.rec_atoms) seen[a] |= 1;
@@ -818,13 +819,32 @@ System::~System() {
   if (graph) cudaGraphExecDestroy(graph);
 }
 
+// Grid points of the three PB grids of one frame, estimated from the atom
+// counts (a sphere at 0.05 atoms/A^3 plus the grid buffer) until a frame
+// has been seen.
+int64_t System::pb_points_estimate() const {
+  int64_t pts = 0;
+  for (int64_t n : {nC, nR, nL}) {
+    if (n == 0) continue;
+    double side = 2.0 * std::cbrt(3.0 * (double)n / (4.0 * kPi * 0.05)) + 2.0 * solv.pb.grid_buffer;
+    double m = side / solv.pb.grid_spacing + 2.0;
+    pts += (int64_t)(m * m * m);
+  }
+  return pts;
+}
+
 int64_t System::footprint(int64_t F) const {
   if (opts.mode == RSTG_MODE_PLAIN) return nC * 200 + F * 0;
+  int64_t pb = 0;
+  if (solv.method == 1) {  // PB pools: ~80 B per solvated and ~30 B per reference grid point
+    int64_t fpb = pb_frames_per_batch > 0 ? std::min(F, pb_frames_per_batch) : std::min<int64_t>(F, 16);
+    pb = fpb * pb_points_estimate() * 110;
+  }
   int64_t per = n_top * 24 + nC * (24 + 16 + 16 + 8 + 8 + 4 + (int64_t)nbr_cap * 4 + 16) + nR * 16 + nL * 16 +
                 (n_res_rec + n_res_lig) * 32 + 256;
   int64_t nb = (nC + kTile - 1) / kTile;
   per += nb * (nb + 1) / 2 * 48 + nb * 32;
-  return per * F + nC * 128;
+  return per * F + nC * 128 + pb;
 }
 
 void System::prepare_fused(const double* x0) {
@@ -1277,6 +1297,76 @@ void System::run_plain(const void* frames, bool f64, bool host_in, int64_t F, rs
   }
 }
 
+void System::run_pb(const void* frames, bool f64, bool host_in, int64_t F, rstg_frame_energy* out, bool host_out) {
+  cudaStream_t st = stream();
+  size_t esz = f64 ? 8 : 4;
+  std::vector<char> hbuf;
+  const char* src = (const char*)frames;
+  if (!host_in) {
+    hbuf.resize((size_t)F * n_top * 3 * esz);
+    RSTG_CUDA(cudaMemcpyAsync(hbuf.data(), frames, hbuf.size(), cudaMemcpyDeviceToHost, st));
+    src = hbuf.data();
+  }
+  std::vector<rstg_frame_energy> res(F);
+  RSTG_CUDA(cudaMemcpyAsync(res.data(), out, F * sizeof(rstg_frame_energy),
+                            host_out ? cudaMemcpyHostToHost : cudaMemcpyDeviceToHost, st));
+  RSTG_CUDA(cudaStreamSynchronize(st));
+  if (!pbe) pbe = std::make_unique<PbBatchEngine>(ctx, st);
+  pbe->set_stream(st);
+  const Topology* T[3] = {&split.complex, &split.rec, &split.lig};
+  const std::vector<int64_t>* sel[3] = {nullptr, &split.rec_atoms, &split.lig_atoms};
+  int64_t chunk = pb_frames_per_batch;
+  if (chunk <= 0) {  // device memory budget: at most 60 % of the free memory and 24 GB
+    size_t fr = 0, tot = 0;
+    RSTG_CUDA(cudaMemGetInfo(&fr, &tot));
+    double budget = std::min(0.6 * (double)fr, 24e9);
+    chunk = std::max<int64_t>(1, (int64_t)(budget / (110.0 * (double)std::max<int64_t>(pb_points_estimate(), 1))));
+  }
+  std::vector<std::vector<double>> xs;
+  std::vector<double> pol;
+  for (int64_t f0 = 0; f0 < F; f0 += chunk) {
+    int64_t B = std::min(chunk, F - f0);
+    xs.assign(B * 3, {});
+    std::vector<const std::vector<double>*> X, Q, R;
+    for (int64_t b = 0; b < B; b++) {
+      std::vector<double> xc(nC * 3);
+      for (int64_t a = 0; a < nC; a++) {
+        int64_t t = split.complex_atoms.empty() ? a : split.complex_atoms[a];
+        for (int d = 0; d < 3; d++) {
+          size_t k = ((size_t)(f0 + b) * n_top + t) * 3 + d;
+          xc[3 * a + d] = f64 ? ((const double*)src)[k] : ((double)((const float*)src)[k] * 0.1) * 10.0;
+        }
+      }
+      for (int k = 0; k < 3; k++) {
+        std::vector<double>& x = xs[3 * b + k];
+        if (!sel[k]) {
+          x = xc;
+        } else {
+          x.resize(sel[k]->size() * 3);
+          for (size_t i = 0; i < sel[k]->size(); i++)
+            for (int d = 0; d < 3; d++) x[3 * i + d] = xc[3 * (*sel[k])[i] + d];
+        }
+        X.push_back(&x);
+        Q.push_back(&T[k]->charges);
+        R.push_back(&T[k]->radii);
+      }
+    }
+    pol.assign(B * 3, 0.0);
+    pb_polar_batch(ctx, st, *pbe, solv.pb, X, Q, R, pol.data(), nullptr);
+    for (int64_t b = 0; b < B; b++) {
+      rstg_frame_energy& e = res[f0 + b];
+      e.complex.polar = pol[3 * b];
+      e.receptor.polar = pol[3 * b + 1];
+      e.ligand.polar = pol[3 * b + 2];
+      e.delta_polar = e.complex.polar - e.receptor.polar - e.ligand.polar;
+      e.delta_total = e.delta_mm + e.delta_polar + e.delta_sa;
+    }
+  }
+  RSTG_CUDA(cudaMemcpyAsync(out, res.data(), F * sizeof(rstg_frame_energy),
+                            host_out ? cudaMemcpyHostToHost : cudaMemcpyHostToDevice, st));
+  RSTG_CUDA(cudaStreamSynchronize(st));
+}
+
 void System::run(const void* frames, bool f64, bool host_in, int64_t F, rstg_frame_energy* out, bool host_out,
                  rstg_residue_energy* decomp_out) {
   if (F <= 0) return;
@@ -1357,7 +1447,10 @@ void System::run(const void* frames, bool f64, bool host_in, int64_t F, rstg_fra
     last_stats[1] = (int64_t)n64;
     last_stats[2] = (int64_t)nre;
     last_stats[3] = h[3];
-    if (h[3] <= nbr_cap) return;
+    if (h[3] <= nbr_cap) {
+      if (solv.method == 1) run_pb(frames, f64, host_in, F, out, host_out);
+      return;
+    }
     // a neighbour list overflowed: grow the capacity and run again
     nbr_cap = ((h[3] * 3 / 2 + 32) + 31) / 32 * 32;
     buf_frames = 0;

@@ -4,6 +4,7 @@
 
 #include "frame_plain.hpp"
 #include "internal.hpp"
+#include "pb_batch.hpp"
 
 namespace rstg {
 
@@ -46,6 +47,10 @@ struct System {
   void* graph_decomp = nullptr;
   int64_t last_stats[4] = {0, 0, 0, 0};
 
+  // fused mode with PB solvation: polar terms from the batched PB engine
+  std::unique_ptr<PbBatchEngine> pbe;
+  int64_t pb_frames_per_batch = 0;  // 0: from the device memory budget
+
   System(Ctx* c, const Topology& t, const std::vector<int64_t>& rres, const std::vector<int64_t>& lres,
          const rstg_solvation& s, const rstg_sa_params& sa, const rstg_system_opts& o);
   ~System();
@@ -76,6 +81,9 @@ struct System {
  private:
   void run_plain(const void* frames, bool f64, bool host_in, int64_t F, rstg_frame_energy* out, bool host_out,
                  rstg_residue_energy* decomp);
+  // PB polar terms of F frames replace the placeholder polar terms in out.
+  void run_pb(const void* frames, bool f64, bool host_in, int64_t F, rstg_frame_energy* out, bool host_out);
+  int64_t pb_points_estimate() const;
   int graph_kernels() const;
 };
 

@@ -732,6 +732,17 @@ class BindingSystem:
         return {"launches": int(st[0]), "fp64_guard_pairs": int(st[1]), "sasa_rechecks": int(st[2]),
                 "neighbour_overflow": int(st[3])}
 
+    def pb_stats(self) -> dict:
+        """Batched PB engine totals of a fused PB system (zeros otherwise)."""
+        st = np.zeros(8)
+        check(N.lib.rstg_system_pb_stats(self._h, _dp(st)))
+        return {"grids": int(st[0]), "cycles": int(st[1]), "fp64_fallbacks": int(st[2]), "ms_setup": st[3],
+                "ms_cycles": st[4], "ms_finish": st[5]}
+
+    def set_pb_batch(self, frames: int) -> None:
+        """Frames per batched PB launch sequence (0: from the memory budget)."""
+        check(N.lib.rstg_system_set_pb_batch(self._h, int(frames)))
+
 
 class Server:
     """Continuous-batching request loop over :class:`BindingSystem` objects."""

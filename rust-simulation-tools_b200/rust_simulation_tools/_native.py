@@ -139,6 +139,8 @@ _sig("rstg_system_footprint", i64, vp, i64)
 _sig("rstg_system_run", C.c_int, vp, fp, i64, P(FrameEnergy), P(ResidueEnergy))
 _sig("rstg_system_run_device", C.c_int, vp, vp, i64, vp, vp)
 _sig("rstg_system_last_stats", C.c_int, vp, ip)
+_sig("rstg_system_pb_stats", C.c_int, vp, dp)
+_sig("rstg_system_set_pb_batch", C.c_int, vp, i64)
 _sig("rstg_system_profile", C.c_int, vp, vp, i64, P(i32), C.c_char_p, dp, dp, dp)
 _sig("rstg_calibrate", C.c_int, C.c_int, dp)
 _sig("rstg_binding_trajectory", C.c_int, vp, vp, cs, cs, i32, ip, i64, ip, i64, P(Solvation), P(SaParams), i64,
