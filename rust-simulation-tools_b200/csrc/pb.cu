@@ -257,9 +257,13 @@ __global__ void k_flood_seed(GeomDev g, const uint8_t* __restrict__ sas, uint8_t
 // 8^3 tiles: inside a tile the front advances until it stops, across tiles
 // through repeated launches until no point changes.  The fixed point is the
 // set of outside-SAS points 6-connected to an outside-SAS boundary point,
-// whatever the visiting order.
-__global__ void k_flood(GeomDev g, const uint8_t* __restrict__ sas, uint8_t* __restrict__ ext, int* changed) {
+// whatever the visiting order.  With act_in, only tiles marked there run; a
+// tile that grew marks itself and its six face neighbours in act_out.
+__global__ void k_flood(GeomDev g, const uint8_t* __restrict__ sas, uint8_t* __restrict__ ext, int* changed,
+                        const uint8_t* __restrict__ act_in, uint8_t* __restrict__ act_out) {
   __shared__ uint8_t se[10][10][10], ss[10][10][10];
+  int tile = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (act_in && !act_in[tile]) return;
   int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
   int bx = blockIdx.x * 8, by = blockIdx.y * 8, bz = blockIdx.z * 8;
   int t = tx + 8 * (ty + 8 * tz);
@@ -289,9 +293,19 @@ __global__ void k_flood(GeomDev g, const uint8_t* __restrict__ sas, uint8_t* __r
     }
     if (!__syncthreads_or(c)) break;
   }
-  if (grew) {
-    ext[ix + (long long)g.nx * (iy + (long long)g.ny * iz)] = 1;
+  if (grew) ext[ix + (long long)g.nx * (iy + (long long)g.ny * iz)] = 1;
+  if (__syncthreads_or(grew) && t == 0) {
     atomicExch(changed, 1);
+    if (act_out) {
+      int X = blockIdx.x, Y = blockIdx.y, Z = blockIdx.z, NX = gridDim.x, NY = gridDim.y, NZ = gridDim.z;
+      act_out[tile] = 1;
+      if (X > 0) act_out[tile - 1] = 1;
+      if (X + 1 < NX) act_out[tile + 1] = 1;
+      if (Y > 0) act_out[tile - NX] = 1;
+      if (Y + 1 < NY) act_out[tile + NX] = 1;
+      if (Z > 0) act_out[tile - NX * NY] = 1;
+      if (Z + 1 < NZ) act_out[tile + NX * NY] = 1;
+    }
   }
 }
 
@@ -801,11 +815,21 @@ static void dielectric_into(Ctx* c, const PbGeom& g, const AtomsDev& A, double p
     k_flood_seed<<<nblk(n, 256), 256, 0, st>>>(gd, sas.as<uint8_t>(), ext.as<uint8_t>());
     launched(c, 2);
     dim3 fb(8, 8, 8), fg(nblk(g.nx, 8), nblk(g.ny, 8), nblk(g.nz, 8));
+    size_t ntile = (size_t)fg.x * fg.y * fg.z;
+    DevBuf act(2 * ntile, st);
+    uint8_t* act_a = act.as<uint8_t>();
+    uint8_t* act_b = act_a + ntile;
     long long limit = (long long)g.nx + g.ny + g.nz + 64;
     bool done = false;
+    int pass = 0;
     for (long long it = 0; it < limit * 8 && !done; it += 8) {
       RSTG_CUDA(cudaMemsetAsync(flag.p, 0, 4, st));
-      for (int k = 0; k < 8; k++) k_flood<<<fg, fb, 0, st>>>(gd, sas.as<uint8_t>(), ext.as<uint8_t>(), flag.as<int>());
+      for (int k = 0; k < 8; k++, pass++) {  // pass 0 visits every tile, later passes the marked ones
+        uint8_t* in = pass == 0 ? nullptr : ((pass & 1) ? act_a : act_b);
+        uint8_t* out = (pass & 1) ? act_b : act_a;
+        RSTG_CUDA(cudaMemsetAsync(out, 0, ntile, st));
+        k_flood<<<fg, fb, 0, st>>>(gd, sas.as<uint8_t>(), ext.as<uint8_t>(), flag.as<int>(), in, out);
+      }
       launched(c, 8);
       int h = 0;
       RSTG_CUDA(cudaMemcpyAsync(&h, flag.p, 4, cudaMemcpyDeviceToHost, st));
@@ -1193,7 +1217,7 @@ void pb_grid_maps(Ctx* c, const std::vector<double>& x, const std::vector<double
       dim3 fb(8, 8, 8), fg(nblk(g.nx, 8), nblk(g.ny, 8), nblk(g.nz, 8));
       for (int guard = 0; guard < 100000; guard++) {
         RSTG_CUDA(cudaMemsetAsync(flag.p, 0, 4, st));
-        k_flood<<<fg, fb, 0, st>>>(gd, sas.as<uint8_t>(), ext.as<uint8_t>(), flag.as<int>());
+        k_flood<<<fg, fb, 0, st>>>(gd, sas.as<uint8_t>(), ext.as<uint8_t>(), flag.as<int>(), nullptr, nullptr);
         launched(c);
         int h = 0;
         RSTG_CUDA(cudaMemcpyAsync(&h, flag.p, 4, cudaMemcpyDeviceToHost, st));

@@ -67,7 +67,7 @@ struct JobD {
 };
 
 struct LvlD {
-  float *e, *e2, *rhs, *res;  // correction (two buffers: a sweep reads one and writes the other)
+  float *e, *rhs, *res;  // correction, right-hand side, residual
   const float *ex, *ey, *ez, *k2;
   int nx, ny, nz, uniform;
   float ih, om, eps, pad;
@@ -99,14 +99,57 @@ __device__ __forceinline__ int wl_job(const WL& w, int b, int& lb) {
   return w.job[lo];
 }
 
+// Level arrays and constants held in registers: reading them through a
+// reference to the descriptor in global memory would make every global store
+// force reloads of the pointers.
+struct Lv {
+  float *__restrict__ e, *__restrict__ rhs, *__restrict__ res;
+  const float *__restrict__ ex, *__restrict__ ey, *__restrict__ ez, *__restrict__ k2;
+  int nx, ny, nz, sy, sz;
+  bool uni;
+  float ih, om, w6;
+};
+__device__ __forceinline__ Lv lv_load(const LvlD* __restrict__ L, int j, int lvl) {
+  const LvlD& d = L[j * kMaxLev + lvl];
+  Lv v;
+  v.e = d.e;
+  v.rhs = d.rhs;
+  v.res = d.res;
+  v.ex = d.ex;
+  v.ey = d.ey;
+  v.ez = d.ez;
+  v.k2 = d.k2;
+  v.nx = d.nx;
+  v.ny = d.ny;
+  v.nz = d.nz;
+  v.sy = d.nx;
+  v.sz = d.nx * d.ny;
+  v.uni = d.uniform != 0;
+  v.ih = d.ih;
+  v.om = d.om;
+  v.w6 = d.eps * d.ih;
+  return v;
+}
+
+// Brick of 32 x 8 x 8 points for a 256-thread block: thread (lane, warp) owns
+// the column (x, y) = (x0 + lane, y0 + warp) over the brick's 8 z planes, so
+// the index arithmetic is done once per block and the 8 points of a column
+// are independent loads in flight together.
+__device__ __forceinline__ void brick_col(int lb, int nx, int ny, int& x, int& y, int& z0) {
+  int ntx = (nx + 31) >> 5, nty = (ny + 7) >> 3;
+  int bx = lb % ntx, t = lb / ntx, by = t % nty, bz = t / nty;
+  x = (bx << 5) + (threadIdx.x & 31);
+  y = (by << 3) + (threadIdx.x >> 5);
+  z0 = bz << 3;
+}
+
 // FP32 7-point stencil of pb_solver.rs:250-317: ns = sum of eps-weighted
 // neighbours, dg = diagonal.
-__device__ __forceinline__ void st32(const LvlD& d, const float* __restrict__ e, int i, int sy, int sz, float& ns,
-                                     float& dg) {
-  if (d.uniform) {
-    float w = d.eps * d.ih;
-    ns = w * ((e[i + 1] + e[i - 1]) + (e[i + sy] + e[i - sy]) + (e[i + sz] + e[i - sz]));
-    dg = 6.0f * w;
+__device__ __forceinline__ void st32(const Lv& d, const float* __restrict__ e, int i, float& ns, float& dg) {
+  const int sy = d.sy, sz = d.sz;
+  if (d.uni) {
+    ns = d.w6 * ((e[i + 1] + e[i - 1]) + (e[i + sy] + e[i - sy]) + (e[i + sz] + e[i - sz]));
+    dg = 6.0f * d.w6;
   } else {
     float a = d.ex[i], b = d.ex[i - 1], c = d.ey[i], dd = d.ey[i - sy], f = d.ez[i], g = d.ez[i - sz];
     ns = ((a * e[i + 1] + b * e[i - 1]) + (c * e[i + sy] + dd * e[i - sy]) + (f * e[i + sz] + g * e[i - sz])) * d.ih;
@@ -116,40 +159,47 @@ __device__ __forceinline__ void st32(const LvlD& d, const float* __restrict__ e,
 
 // FP64 residual r = 4 pi ec rho + ns - dg phi at the interior points; r is
 // stored rounded to FP32 as the level-0 right-hand side and its squares are
-// summed per block (fixed order) for the RMS test.
-__global__ void k_res64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L, const JobState* __restrict__ S,
-                        int want, double* __restrict__ part, int nparts) {
+// summed per brick (fixed order) for the RMS test.
+__global__ void __launch_bounds__(256) k_res64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
+                                               const JobState* __restrict__ S, int want, double* __restrict__ part,
+                                               int nparts) {
   __shared__ double sh[32];
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != want) return;
   const JobD& d = J[j];
-  float* rhs0 = L[j * kMaxLev].rhs;
-  int nxi = d.nx - 2, nyi = d.ny - 2;
-  int cnt = nxi * nyi * (d.nz - 2);
-  int k = lb * blockDim.x + threadIdx.x;
+  float* __restrict__ rhs0 = L[j * kMaxLev].rhs;
+  const double* __restrict__ p = d.phi;
+  const double* __restrict__ rho = d.rho;
+  const double *__restrict__ ex = d.ex, *__restrict__ ey = d.ey, *__restrict__ ez = d.ez, *__restrict__ kk = d.k2;
+  const bool uni = d.uniform != 0;
+  const double ih = d.ih, wt = d.eps * d.ih;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny;
+  int x, y, z0;
+  brick_col(lb, nx, ny, x, y, z0);
   double acc = 0.0;
-  if (k < cnt) {
-    int ix = 1 + k % nxi, row = k / nxi;
-    int iy = 1 + row % nyi, iz = 1 + row / nyi;
-    int sy = d.nx, sz = d.nx * d.ny, i = ix + sy * iy + sz * iz;
-    const double* p = d.phi;
-    double ns, dg;
-    if (d.uniform) {
-      double wt = d.eps * d.ih;
-      ns = wt * ((p[i + 1] + p[i - 1]) + (p[i + sy] + p[i - sy]) + (p[i + sz] + p[i - sz]));
-      dg = 6.0 * wt;
-    } else {
-      double a = d.ex[i], b = d.ex[i - 1], c = d.ey[i], dd = d.ey[i - sy], f = d.ez[i], g = d.ez[i - sz];
-      ns = (a * p[i + 1] + b * p[i - 1]) * d.ih + (c * p[i + sy] + dd * p[i - sy]) * d.ih +
-           (f * p[i + sz] + g * p[i - sz]) * d.ih;
-      dg = (a + b) * d.ih + (c + dd) * d.ih + (f + g) * d.ih + d.k2[i];
+  if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      int z = z0 + k;
+      if (z < 1 || z > nz - 2) continue;
+      int i = x + sy * y + sz * z;
+      double ns, dg;
+      if (uni) {
+        ns = wt * ((p[i + 1] + p[i - 1]) + (p[i + sy] + p[i - sy]) + (p[i + sz] + p[i - sz]));
+        dg = 6.0 * wt;
+      } else {
+        double a = ex[i], b = ex[i - 1], c = ey[i], dd = ey[i - sy], f = ez[i], g = ez[i - sz];
+        ns = (a * p[i + 1] + b * p[i - 1]) * ih + (c * p[i + sy] + dd * p[i - sy]) * ih +
+             (f * p[i + sz] + g * p[i - sz]) * ih;
+        dg = (a + b) * ih + (c + dd) * ih + (f + g) * ih + kk[i];
+      }
+      double r = kFourPiEcB * rho[i] + ns - dg * p[i];
+      rhs0[i] = (float)r;
+      acc += r * r;
     }
-    double r = kFourPiEcB * d.rho[i] + ns - dg * p[i];
-    rhs0[i] = (float)r;
-    acc = r * r;
   }
-  double s = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[(long long)j * nparts + lb] = s;
+  double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[(long long)j * nparts + lb] = t;
 }
 
 // RMS of the residual and the reference's multigrid bookkeeping
@@ -160,7 +210,7 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
   int j = w.job[blockIdx.x];
   if (S[j].status != kMg) return;
   const JobD& d = J[j];
-  int used = (int)(((long long)(d.nx - 2) * (d.ny - 2) * (d.nz - 2) + kT - 1) / kT);
+  int used = ((d.nx + 31) >> 5) * ((d.ny + 7) >> 3) * ((d.nz + 7) >> 3);
   double s = 0.0;
   for (int k = threadIdx.x; k < used; k += blockDim.x) s += part[(long long)j * nparts + k];
   s = block_sum(s, sh);
@@ -194,132 +244,58 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
 }
 
 // phi += e over every point (the prolongation can reach boundary points of
-// grids with even dimensions), then e = 0 for the next cycle.
-__global__ void k_update64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
-                           const JobState* __restrict__ S, int want) {
+// grids with even dimensions), then e = 0 for the next cycle; four points
+// per thread (phi and e start on 64-element boundaries).
+__global__ void __launch_bounds__(256) k_update64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
+                                                  const JobState* __restrict__ S, int want) {
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != want) return;
   const JobD& d = J[j];
-  float* e0 = L[j * kMaxLev].e;
+  float* __restrict__ e0 = L[j * kMaxLev].e;
+  double* __restrict__ phi = d.phi;
   int n = d.nx * d.ny * d.nz;
-  int i = lb * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  d.phi[i] += (double)e0[i];
-  e0[i] = 0.0f;
-}
-
-// One red-black SOR sweep (colour 0, then colour 1; pb_solver.rs:250-317) on
-// a brick of 32 x 8 x 8 points of one level.  The brick's correction and a
-// ring of two points around it are staged in shared memory; colour 0 is
-// relaxed on the brick and the first ring, then colour 1 on the brick,
-// whose colour-0 neighbours are then final.  Reading src and writing dst
-// keeps the bricks independent, so the level's maps and right-hand side are
-// read from DRAM once per sweep instead of once per colour (the overlapping
-// rings are served by L2).  Boundary points are copied.
-constexpr int kBX = 32, kBY = 8, kBZ = 8, kPX = kBX + 4, kPY = kBY + 4, kPZ = kBZ + 4;
-
-// Relaxes point x of a row (smem index s, global index i) in place.
-__device__ __forceinline__ void relax_pt(const LvlD& d, float* __restrict__ sm, int s, int i, int sy, int sz,
-                                         bool uni, float w6, float ih, float om, const float* __restrict__ rhs) {
-  constexpr int P = kPX * kPY;
-  float ns, dg;
-  if (uni) {
-    ns = w6 * ((sm[s + 1] + sm[s - 1]) + (sm[s + kPX] + sm[s - kPX]) + (sm[s + P] + sm[s - P]));
-    dg = 6.0f * w6;
+  int i = 4 * (lb * blockDim.x + threadIdx.x);
+  if (i + 3 < n) {
+    float4 e = *(const float4*)(e0 + i);
+    double2 a = *(const double2*)(phi + i), b = *(const double2*)(phi + i + 2);
+    a.x += (double)e.x;
+    a.y += (double)e.y;
+    b.x += (double)e.z;
+    b.y += (double)e.w;
+    *(double2*)(phi + i) = a;
+    *(double2*)(phi + i + 2) = b;
+    *(float4*)(e0 + i) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   } else {
-    float a = d.ex[i], b = d.ex[i - 1], c = d.ey[i], e = d.ey[i - sy], f = d.ez[i], g = d.ez[i - sz];
-    ns = ((a * sm[s + 1] + b * sm[s - 1]) + (c * sm[s + kPX] + e * sm[s - kPX]) + (f * sm[s + P] + g * sm[s - P])) *
-         ih;
-    dg = ((a + b) + (c + e) + (f + g)) * ih + d.k2[i];
+    for (int k = i; k < n; k++) {
+      phi[k] += (double)e0[k];
+      e0[k] = 0.0f;
+    }
   }
-  float old = sm[s];
-  float gs = __fdividef(ns + rhs[i], dg);
-  sm[s] = old + om * (gs - old);
 }
 
-__global__ void __launch_bounds__(256) k_sweep32(WL w, const LvlD* __restrict__ L, int lvl,
-                                                 const JobState* __restrict__ S, int src) {
-  __shared__ float sm[kPZ * kPY * kPX];
+// One colour of a red-black SOR sweep on one level (pb_solver.rs:250-317),
+// one point of the colour per thread.  Each colour pass streams the level's
+// arrays once; at the batch sizes used here this runs at the HBM copy rate,
+// which a single-pass (both colours) brick with halo staging did not reach.
+__global__ void __launch_bounds__(256) k_rb32(WL w, const LvlD* __restrict__ L, int lvl,
+                                              const JobState* __restrict__ S, int colour) {
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != kMg) return;
-  const LvlD& d = L[j * kMaxLev + lvl];
-  const float* __restrict__ ein = src ? d.e2 : d.e;
-  float* __restrict__ eout = src ? d.e : d.e2;
-  const float* __restrict__ rhs = d.rhs;
-  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny;
-  const int ntx = (nx + kBX - 1) / kBX, nty = (ny + kBY - 1) / kBY;
-  const int x0 = (lb % ntx) * kBX, y0 = ((lb / ntx) % nty) * kBY, z0 = (lb / (ntx * nty)) * kBZ;
-  const float om = d.om, ih = d.ih, w6 = d.eps * d.ih;
-  const bool uni = d.uniform;
-  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-  // stage the brick and a ring of two points: one warp per row of 36
-  {
-    constexpr int NR = kPY * kPZ / 8;  // rows per warp
-    float v[NR], u[NR];
-    const int xa = x0 - 2 + lane, xb = x0 + 30 + lane;
-#pragma unroll
-    for (int k = 0; k < NR; k++) {
-      int r = wp + 8 * k;
-      int y = y0 + r % kPY - 2, z = z0 + r / kPY - 2;
-      bool rok = y >= 0 && y < ny && z >= 0 && z < nz;
-      int base = sy * y + sz * z;
-      v[k] = (rok && xa >= 0 && xa < nx) ? ein[base + xa] : 0.0f;
-      u[k] = (rok && lane < 4 && xb < nx) ? ein[base + xb] : 0.0f;
-    }
-#pragma unroll
-    for (int k = 0; k < NR; k++) {
-      int r = wp + 8 * k;
-      sm[r * kPX + lane] = v[k];
-      if (lane < 4) sm[r * kPX + 32 + lane] = u[k];
-    }
-  }
-  __syncthreads();
-  // colour 0 ((x + y + z) even) on the brick and its first ring: rows of the
-  // ring-1 cross-section, 16 points inside the brick per row (half a warp)
-  {
-    const int hl = lane & 15, half = lane >> 4;
-#pragma unroll
-    for (int r = 2 * wp + half; r < (kBY + 2) * (kBZ + 2); r += 16) {
-      int ly = r % (kBY + 2) - 1, lz = r / (kBY + 2) - 1;
-      int y = y0 + ly, z = z0 + lz;
-      if (y < 1 || y > ny - 2 || z < 1 || z > nz - 2) continue;
-      int x = x0 + ((x0 + y + z) & 1) + 2 * hl;
-      if (x >= 1 && x <= nx - 2)
-        relax_pt(d, sm, (x - x0 + 2) + kPX * ((ly + 2) + kPY * (lz + 2)), x + sy * y + sz * z, sy, sz, uni, w6, ih, om,
-                 rhs);
-    }
-    // the colour-0 point of each row just outside the brick in x (x0 - 1 or x0 + 32)
-    for (int r = threadIdx.x; r < (kBY + 2) * (kBZ + 2); r += 256) {
-      int ly = r % (kBY + 2) - 1, lz = r / (kBY + 2) - 1;
-      int y = y0 + ly, z = z0 + lz;
-      if (y < 1 || y > ny - 2 || z < 1 || z > nz - 2) continue;
-      int x = ((x0 - 1 + y + z) & 1) == 0 ? x0 - 1 : x0 + kBX;
-      if (x >= 1 && x <= nx - 2)
-        relax_pt(d, sm, (x - x0 + 2) + kPX * ((ly + 2) + kPY * (lz + 2)), x + sy * y + sz * z, sy, sz, uni, w6, ih, om,
-                 rhs);
-    }
-  }
-  __syncthreads();
-  // colour 1 on the brick
-  {
-    const int hl = lane & 15, half = lane >> 4;
-#pragma unroll
-    for (int r = 2 * wp + half; r < kBY * kBZ; r += 16) {
-      int ly = r % kBY, lz = r / kBY;
-      int y = y0 + ly, z = z0 + lz;
-      if (y < 1 || y > ny - 2 || z < 1 || z > nz - 2) continue;
-      int x = x0 + ((x0 + y + z + 1) & 1) + 2 * hl;
-      if (x >= 1 && x <= nx - 2)
-        relax_pt(d, sm, (x - x0 + 2) + kPX * ((ly + 2) + kPY * (lz + 2)), x + sy * y + sz * z, sy, sz, uni, w6, ih, om,
-                 rhs);
-    }
-  }
-  __syncthreads();
-  for (int r = wp; r < kBY * kBZ; r += 8) {
-    int ly = r % kBY, lz = r / kBY;
-    int x = x0 + lane, y = y0 + ly, z = z0 + lz;
-    if (x < nx && y < ny && z < nz) eout[x + sy * y + sz * z] = sm[(lane + 2) + kPX * ((ly + 2) + kPY * (lz + 2))];
-  }
+  const Lv d = lv_load(L, j, lvl);
+  int hw = (d.nx - 1) >> 1, nyi = d.ny - 2;
+  int cnt = hw * nyi * (d.nz - 2);
+  int k = lb * blockDim.x + threadIdx.x;
+  if (k >= cnt) return;
+  int t = k % hw, row = k / hw;
+  int iy = 1 + row % nyi, iz = 1 + row / nyi;
+  int ix = 1 + ((1 + iy + iz + colour) & 1) + 2 * t;
+  if (ix >= d.nx - 1) return;
+  int i = ix + d.sy * iy + d.sz * iz;
+  float ns, dg;
+  st32(d, d.e, i, ns, dg);
+  float old = d.e[i];
+  float gs = __fdividef(ns + d.rhs[i], dg);
+  d.e[i] = old + d.om * (gs - old);
 }
 
 // One colour of the plain SOR sweep (pb_solver.rs:373-447) on the level-0
@@ -329,7 +305,7 @@ __global__ void k_sor32(WL w, const LvlD* __restrict__ L, const JobState* __rest
   __shared__ double sh[32];
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != kSor) return;
-  const LvlD& d = L[j * kMaxLev];
+  const Lv d = lv_load(L, j, 0);
   float om = (float)S[j].om;
   int hw = (d.nx - 1) >> 1, nyi = d.ny - 2;
   int cnt = hw * nyi * (d.nz - 2);
@@ -340,9 +316,9 @@ __global__ void k_sor32(WL w, const LvlD* __restrict__ L, const JobState* __rest
     int iy = 1 + row % nyi, iz = 1 + row / nyi;
     int ix = 1 + ((1 + iy + iz + colour) & 1) + 2 * t;
     if (ix < d.nx - 1) {
-      int sy = d.nx, sz = d.nx * d.ny, i = ix + sy * iy + sz * iz;
+      int i = ix + d.sy * iy + d.sz * iz;
       float ns, dg;
-      st32(d, d.e, i, sy, sz, ns, dg);
+      st32(d, d.e, i, ns, dg);
       float old = d.e[i];
       float gs = (ns + d.rhs[i]) / dg;
       float dv = gs - old;
@@ -384,97 +360,204 @@ __global__ void k_sor_norm(WL w, const JobD* __restrict__ J, JobState* __restric
     t.status = kSorCap;
 }
 
-__global__ void k_res32(WL w, const LvlD* __restrict__ L, int lvl, const JobState* __restrict__ S) {
+__global__ void __launch_bounds__(256) k_res32(WL w, const LvlD* __restrict__ L, int lvl,
+                                               const JobState* __restrict__ S) {
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != kMg) return;
-  const LvlD& d = L[j * kMaxLev + lvl];
-  int nxi = d.nx - 2, nyi = d.ny - 2;
-  int cnt = nxi * nyi * (d.nz - 2);
-  int k = lb * blockDim.x + threadIdx.x;
-  if (k >= cnt) return;
-  int ix = 1 + k % nxi, row = k / nxi;
-  int iy = 1 + row % nyi, iz = 1 + row / nyi;
-  int sy = d.nx, sz = d.nx * d.ny, i = ix + sy * iy + sz * iz;
-  float ns, dg;
-  st32(d, d.e2, i, sy, sz, ns, dg);
-  d.res[i] = d.rhs[i] + ns - dg * d.e2[i];
+  const Lv d = lv_load(L, j, lvl);
+  int x, y, z0;
+  brick_col(lb, d.nx, d.ny, x, y, z0);
+  if (x < 1 || x > d.nx - 2 || y < 1 || y > d.ny - 2) return;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    int z = z0 + k;
+    if (z < 1 || z > d.nz - 2) continue;
+    int i = x + d.sy * y + d.sz * z;
+    float ns, dg;
+    st32(d, d.e, i, ns, dg);
+    d.res[i] = d.rhs[i] + ns - dg * d.e[i];
+  }
 }
 
 // Full-weighting restriction x 0.25 of the level-l residual into the
 // level-(l+1) right-hand side (pb_solver.rs:459-520); the coarse correction
 // starts from zero.
-__global__ void k_restrict32(WL w, const LvlD* __restrict__ L, int lvl, const JobState* __restrict__ S) {
+__global__ void __launch_bounds__(256) k_restrict32(WL w, const LvlD* __restrict__ L, int lvl,
+                                                    const JobState* __restrict__ S) {
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != kMg) return;
-  const LvlD& f = L[j * kMaxLev + lvl];
-  const LvlD& c = L[j * kMaxLev + lvl + 1];
-  int cn = c.nx * c.ny * c.nz;
-  int i = lb * blockDim.x + threadIdx.x;
-  if (i >= cn) return;
-  int cx = i % c.nx, cy = (i / c.nx) % c.ny, cz = i / (c.nx * c.ny);
-  int fx = 2 * cx, fy = 2 * cy, fz = 2 * cz;
-  float sum = 0.0f, ws = 0.0f;
-  for (int dz = -1; dz <= 1; dz++)
-    for (int dy = -1; dy <= 1; dy++)
-      for (int dx = -1; dx <= 1; dx++) {
-        int x = fx + dx, y = fy + dy, z = fz + dz;
-        if (x < 0 || x >= f.nx || y < 0 || y >= f.ny || z < 0 || z >= f.nz) continue;
-        float wt = (dx == 0 ? 2.0f : 1.0f) * (dy == 0 ? 2.0f : 1.0f) * (dz == 0 ? 2.0f : 1.0f);
-        sum += wt * f.res[x + f.nx * (y + f.ny * z)];
-        ws += wt;
+  const Lv f = lv_load(L, j, lvl), c = lv_load(L, j, lvl + 1);
+  int cx, cy, cz0;
+  brick_col(lb, c.nx, c.ny, cx, cy, cz0);
+  if (cx >= c.nx || cy >= c.ny) return;
+  const float* __restrict__ res = f.res;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    int cz = cz0 + k;
+    if (cz >= c.nz) continue;
+    int fx = 2 * cx, fy = 2 * cy, fz = 2 * cz;
+    float sum = 0.0f, ws = 0.0f;
+    for (int dz = -1; dz <= 1; dz++) {
+      int z = fz + dz;
+      if (z < 0 || z >= f.nz) continue;
+      float wz = dz == 0 ? 2.0f : 1.0f;
+      for (int dy = -1; dy <= 1; dy++) {
+        int y = fy + dy;
+        if (y < 0 || y >= f.ny) continue;
+        float wyz = wz * (dy == 0 ? 2.0f : 1.0f);
+        for (int dx = -1; dx <= 1; dx++) {
+          int x = fx + dx;
+          if (x < 0 || x >= f.nx) continue;
+          float wt = wyz * (dx == 0 ? 2.0f : 1.0f);
+          sum += wt * res[x + f.sy * y + f.sz * z];
+          ws += wt;
+        }
       }
-  c.rhs[i] = 0.25f * sum / ws;
-  c.e[i] = 0.0f;
+    }
+    int i = cx + c.sy * cy + c.sz * cz;
+    c.rhs[i] = 0.25f * sum / ws;
+    c.e[i] = 0.0f;
+  }
 }
 
 // Trilinear prolongation of the level-(l+1) correction added at every
-// level-l point (pb_solver.rs:522-578), into the pre-smoothed correction.
-__global__ void k_prolong32(WL w, const LvlD* __restrict__ L, int lvl, const JobState* __restrict__ S) {
+// level-l point (pb_solver.rs:522-578).
+__global__ void __launch_bounds__(256) k_prolong32(WL w, const LvlD* __restrict__ L, int lvl,
+                                                   const JobState* __restrict__ S) {
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != kMg) return;
-  const LvlD& f = L[j * kMaxLev + lvl];
-  const LvlD& c = L[j * kMaxLev + lvl + 1];
-  int fn = f.nx * f.ny * f.nz;
-  int i = lb * blockDim.x + threadIdx.x;
-  if (i >= fn) return;
-  int fx = i % f.nx, fy = (i / f.nx) % f.ny, fz = i / (f.nx * f.ny);
-  float cxf = (float)fx * 0.5f, cyf = (float)fy * 0.5f, czf = (float)fz * 0.5f;
+  const Lv f = lv_load(L, j, lvl), c = lv_load(L, j, lvl + 1);
+  int fx, fy, fz0;
+  brick_col(lb, f.nx, f.ny, fx, fy, fz0);
+  if (fx >= f.nx || fy >= f.ny) return;
+  const float* __restrict__ ce = c.e;
   int mx = c.nx >= 2 ? c.nx - 2 : 0, my = c.ny >= 2 ? c.ny - 2 : 0, mz = c.nz >= 2 ? c.nz - 2 : 0;
-  int x0 = min(fx >> 1, mx), y0 = min(fy >> 1, my), z0 = min(fz >> 1, mz);
-  float dx = cxf - (float)x0, dy = cyf - (float)y0, dz = czf - (float)z0;
-  const float* ce = c.e;
-  auto at = [&](int x, int y, int z) { return ce[x + c.nx * (y + c.ny * z)]; };
-  float c00 = at(x0, y0, z0) * (1.0f - dx) + at(x0 + 1, y0, z0) * dx;
-  float c10 = at(x0, y0 + 1, z0) * (1.0f - dx) + at(x0 + 1, y0 + 1, z0) * dx;
-  float c01 = at(x0, y0, z0 + 1) * (1.0f - dx) + at(x0 + 1, y0, z0 + 1) * dx;
-  float c11 = at(x0, y0 + 1, z0 + 1) * (1.0f - dx) + at(x0 + 1, y0 + 1, z0 + 1) * dx;
-  float c0 = c00 * (1.0f - dy) + c10 * dy, c1 = c01 * (1.0f - dy) + c11 * dy;
-  f.e2[i] += c0 * (1.0f - dz) + c1 * dz;
+  int x0 = min(fx >> 1, mx), y0 = min(fy >> 1, my);
+  float dx = (float)fx * 0.5f - (float)x0, dy = (float)fy * 0.5f - (float)y0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    int fz = fz0 + k;
+    if (fz >= f.nz) continue;
+    int z0 = min(fz >> 1, mz);
+    float dz = (float)fz * 0.5f - (float)z0;
+    const float* b = ce + x0 + c.sy * y0 + c.sz * z0;
+    float c00 = b[0] * (1.0f - dx) + b[1] * dx;
+    float c10 = b[c.sy] * (1.0f - dx) + b[c.sy + 1] * dx;
+    float c01 = b[c.sz] * (1.0f - dx) + b[c.sz + 1] * dx;
+    float c11 = b[c.sz + c.sy] * (1.0f - dx) + b[c.sz + c.sy + 1] * dx;
+    float c0 = c00 * (1.0f - dy) + c10 * dy, c1 = c01 * (1.0f - dy) + c11 * dy;
+    f.e[fx + f.sy * fy + f.sz * fz] += c0 * (1.0f - dz) + c1 * dz;
+  }
 }
 
 // Coarsest level: 50 red-black sweeps in one block per grid (pb_solver.rs:850-870).
 __global__ void k_coarse32(WL w, const LvlD* __restrict__ L, int lvl, const JobState* __restrict__ S, int sweeps) {
   int j = w.job[blockIdx.x];
   if (S[j].status != kMg) return;
-  const LvlD& d = L[j * kMaxLev + lvl];
+  const Lv d = lv_load(L, j, lvl);
   if (d.nx < 3 || d.ny < 3 || d.nz < 3) return;
   int nxi = d.nx - 2, nyi = d.ny - 2;
   int ni = nxi * nyi * (d.nz - 2);
-  int sy = d.nx, sz = d.nx * d.ny;
   for (int s = 0; s < sweeps; s++)
     for (int colour = 0; colour < 2; colour++) {
       for (int k = threadIdx.x; k < ni; k += blockDim.x) {
         int ix = 1 + k % nxi, iy = 1 + (k / nxi) % nyi, iz = 1 + k / (nxi * nyi);
         if (((ix + iy + iz + colour) & 1) != 0) continue;
-        int i = ix + sy * iy + sz * iz;
+        int i = ix + d.sy * iy + d.sz * iz;
         float ns, dg;
-        st32(d, d.e, i, sy, sz, ns, dg);
+        st32(d, d.e, i, ns, dg);
         float old = d.e[i];
         float gs = (ns + d.rhs[i]) / dg;
         d.e[i] = old + d.om * (gs - old);
       }
       __syncthreads();
     }
+}
+
+// Debye-Hueckel boundary values (set_dh_boundary, pb_solver.rs:68-93) of
+// every grid of a batch in one launch: per boundary point the sum over atoms
+// of 332.0522 q exp(-kappa r) / (eps_out r), pair terms in FP32 (coordinates
+// relative to the grid origin), accumulated in FP64.  Reference grids
+// (kappa = 0) skip the exponential.
+struct DhD {
+  double* phi;
+  const double *xyz, *q;
+  int nx, ny, nz, na;
+  double ox, oy, oz, h, kap, eout;
+};
+
+// Boundary points enumerated face by face: the two z faces, the two y faces
+// of the interior z planes, the two x faces of the interior rows.
+__device__ __forceinline__ bool bnd_point(int nx, int ny, int nz, long long k, int& ix, int& iy, int& iz) {
+  long long nxy = (long long)nx * ny;
+  int nzi = max(nz - 2, 0), nyi = max(ny - 2, 0);
+  if (k < 2 * nxy) {
+    iz = k < nxy ? 0 : nz - 1;
+    long long r = k % nxy;
+    ix = (int)(r % nx);
+    iy = (int)(r / nx);
+    return true;
+  }
+  k -= 2 * nxy;
+  long long nyf = (long long)nx * nzi;
+  if (k < 2 * nyf) {
+    iy = k < nyf ? 0 : ny - 1;
+    long long r = k % nyf;
+    ix = (int)(r % nx);
+    iz = 1 + (int)(r / nx);
+    return true;
+  }
+  k -= 2 * nyf;
+  long long nxf = (long long)nyi * nzi;
+  if (k < 2 * nxf) {
+    ix = k < nxf ? 0 : nx - 1;
+    long long r = k % nxf;
+    iy = 1 + (int)(r % nyi);
+    iz = 1 + (int)(r / nyi);
+    return true;
+  }
+  return false;
+}
+
+long long bnd_count(const PbGeom& g) {
+  long long nzi = std::max(g.nz - 2, 0), nyi = std::max(g.ny - 2, 0);
+  return 2LL * g.nx * g.ny + 2LL * g.nx * nzi + 2LL * nyi * nzi;
+}
+
+__global__ void __launch_bounds__(256) k_dh32(WL w, const DhD* __restrict__ D) {
+  __shared__ float4 sa[256];
+  int lb, j = wl_job(w, blockIdx.x, lb);
+  const DhD& d = D[j];
+  long long nb = 2LL * d.nx * d.ny + 2LL * d.nx * max(d.nz - 2, 0) + 2LL * max(d.ny - 2, 0) * max(d.nz - 2, 0);
+  long long k = (long long)lb * blockDim.x + threadIdx.x;
+  int ix = 0, iy = 0, iz = 0;
+  bool valid = k < nb && bnd_point(d.nx, d.ny, d.nz, k, ix, iy, iz);
+  float px = (float)(ix * d.h), py = (float)(iy * d.h), pz = (float)(iz * d.h);
+  float kap = (float)d.kap;
+  bool ionic = d.kap != 0.0;
+  double acc = 0.0;
+  for (int a0 = 0; a0 < d.na; a0 += 256) {
+    int a = a0 + threadIdx.x;
+    if (a < d.na)
+      sa[threadIdx.x] = make_float4((float)(d.xyz[3 * a] - d.ox), (float)(d.xyz[3 * a + 1] - d.oy),
+                                    (float)(d.xyz[3 * a + 2] - d.oz), (float)d.q[a]);
+    __syncthreads();
+    int m = min(256, d.na - a0);
+    if (valid) {
+      for (int t = 0; t < m; t++) {
+        float4 A = sa[t];
+        float dx = px - A.x, dy = py - A.y, dz = pz - A.z;
+        float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= 1e-20f) continue;
+        float ir = rsqrtf(r2);
+        float term = A.w * ir;
+        if (ionic) term *= __expf(-kap * (r2 * ir));
+        acc += (double)term;
+      }
+    }
+    __syncthreads();
+  }
+  if (valid) d.phi[ix + (long long)d.nx * (iy + (long long)d.ny * iz)] = 332.0522 * acc / d.eout;
 }
 
 // Level-0 FP32 maps from the FP64 maps, then injection to coarser levels
@@ -556,6 +639,7 @@ __global__ void k_maxabs64(const JobD* __restrict__ J, double* __restrict__ M) {
 }
 
 long long cdiv(long long n, int t) { return (n + t - 1) / t; }
+long long nbricks(const PbGeom& g) { return cdiv(g.nx, 32) * cdiv(g.ny, 8) * cdiv(g.nz, 8); }
 
 // Host-side work lists: per launch slot the listed grids and their first
 // blocks, packed into one device buffer.
@@ -569,11 +653,11 @@ struct Lists {
     slots.emplace_back();
     return (int)slots.size() - 1;
   }
-  void add(int s, int j, long long blocks) {
+  void add(int s, long long j, long long blocks) {
     if (blocks <= 0) return;
     Slot& S = slots[s];
     S.start.push_back(S.total);
-    S.job.push_back(j);
+    S.job.push_back((int)j);
     S.total += (int)blocks;
   }
   // Uploads every slot; wl[s] receives the device view.
@@ -633,6 +717,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     size_t n = J.g.n();
     Y.o64 = n64;
     n64 += (J.uniform ? 2 : 6) * n;
+    n64 = (n64 + 63) & ~(size_t)63;
     PbGeom g = J.g;
     Y.lv[0] = g;
     int nl = 0;
@@ -654,7 +739,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     for (int l = 0; l <= std::max(nl, 0); l++) {
       Y.o32[l] = n32;
       size_t m = Y.lv[l].n();
-      n32 += (J.uniform ? 4 : 8) * m;
+      n32 += (J.uniform ? 3 : 7) * m;
       n32 = (n32 + 63) & ~(size_t)63;
     }
   }
@@ -675,7 +760,46 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
            *ez = J.uniform ? nullptr : base + 4 * n, *k2 = J.uniform ? nullptr : base + 5 * n;
     pb_maps_into(c_, J.g, *J.atoms, p, J.ein, J.eout, J.kap, J.ionic, rho, ex, ey, ez, k2);
     RSTG_CUDA(cudaMemsetAsync(phi, 0, n * 8, st));
-    pb_boundary(c_, J.g, phi, *J.atoms, J.bc);
+    if (J.bc.kind != 1) pb_boundary(c_, J.g, phi, *J.atoms, J.bc);
+  }
+  // Debye-Hueckel boundary values of the listed grids in one launch
+  auto dh_launch = [&](const std::vector<int>& which) {
+    std::vector<DhD> dd;
+    Lists dl;
+    int sd = dl.add_slot();
+    for (int j : which) {
+      const PbJob& J = jobs[j];
+      DhD x;
+      x.phi = P64 + lay[j].o64;
+      x.xyz = J.atoms->xyz.as<double>();
+      x.q = J.atoms->q.as<double>();
+      x.nx = J.g.nx;
+      x.ny = J.g.ny;
+      x.nz = J.g.nz;
+      x.na = J.atoms->n;
+      x.ox = J.g.ox;
+      x.oy = J.g.oy;
+      x.oz = J.g.oz;
+      x.h = J.g.h;
+      x.kap = J.bc.kappa;
+      x.eout = J.bc.eout;
+      dl.add(sd, (long long)dd.size(), cdiv(bnd_count(J.g), 256));
+      dd.push_back(x);
+    }
+    if (dd.empty()) return;
+    DevBuf dbuf(dd.size() * sizeof(DhD), st);
+    RSTG_CUDA(cudaMemcpyAsync(dbuf.p, dd.data(), dd.size() * sizeof(DhD), cudaMemcpyHostToDevice, st));
+    std::vector<WL> wl;
+    dl.upload(lists_, st, wl);
+    k_dh32<<<dl.slots[sd].total, 256, 0, st>>>(wl[sd], dbuf.as<DhD>());
+    launched(c_);
+    RSTG_CUDA(cudaStreamSynchronize(st));  // dd is pageable and goes out of scope
+  };
+  {
+    std::vector<int> which;
+    for (int j = 0; j < nj; j++)
+      if (jobs[j].bc.kind == 1) which.push_back(j);
+    dh_launch(which);
   }
 
   // ---- descriptors ----------------------------------------------------------
@@ -722,7 +846,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     s.best = s.prev = DBL_MAX;
     s.om = 1.0;
     s.status = Y.nlev >= 0 ? kMg : kSor;
-    max_res = std::max(max_res, cdiv((long long)(J.g.nx - 2) * (J.g.ny - 2) * (J.g.nz - 2), kT));
+    max_res = std::max(max_res, nbricks(J.g));
     max_sor = std::max(max_sor, cdiv((long long)((J.g.nx - 1) / 2) * (J.g.ny - 2) * (J.g.nz - 2), kT));
     for (int l = 0; l <= std::max(Y.nlev, 0); l++) {
       const PbGeom& g = Y.lv[l];
@@ -731,14 +855,13 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       std::memset(&L, 0, sizeof(L));
       float* b = P32 + Y.o32[l];
       L.e = b;
-      L.e2 = b + m;
-      L.rhs = b + 2 * m;
-      L.res = b + 3 * m;
+      L.rhs = b + m;
+      L.res = b + 2 * m;
       if (!J.uniform) {
-        L.ex = b + 4 * m;
-        L.ey = b + 5 * m;
-        L.ez = b + 6 * m;
-        L.k2 = b + 7 * m;
+        L.ex = b + 3 * m;
+        L.ey = b + 4 * m;
+        L.ez = b + 5 * m;
+        L.k2 = b + 6 * m;
       }
       L.nx = g.nx;
       L.ny = g.ny;
@@ -801,7 +924,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     int s = init.add_slot(), sn = init.add_slot();
     for (int j = 0; j < nj; j++)
       if (hs[j].status == kMg) {
-        init.add(s, j, cdiv((long long)(jobs[j].g.nx - 2) * (jobs[j].g.ny - 2) * (jobs[j].g.nz - 2), kT));
+        init.add(s, j, nbricks(jobs[j].g));
         init.add(sn, j, 1);
       }
     if (init.slots[s].total > 0) {
@@ -833,10 +956,11 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       if (any_mg) {
         for (int l = 0; l <= maxlev; l++) {
           if (go(ls[l].rb)) {
-            for (int s = 0; s < 3; s++) {  // e -> e2 -> e -> e2
-              k_sweep32<<<go(ls[l].rb), 256, 0, st>>>(wl[ls[l].rb], dL, l, dS, s & 1);
-              n++;
-            }
+            for (int s = 0; s < 3; s++)
+              for (int colour = 0; colour < 2; colour++) {
+                k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour);
+                n++;
+              }
             k_res32<<<go(ls[l].res), kT, 0, st>>>(wl[ls[l].res], dL, l, dS);
             k_restrict32<<<go(ls[l].restr), kT, 0, st>>>(wl[ls[l].restr], dL, l, dS);
             n += 2;
@@ -850,10 +974,11 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           if (!go(ls[l].prol)) continue;
           k_prolong32<<<go(ls[l].prol), kT, 0, st>>>(wl[ls[l].prol], dL, l, dS);
           n++;
-          for (int s = 0; s < 3; s++) {  // e2 -> e -> e2 -> e
-            k_sweep32<<<go(ls[l].rb), 256, 0, st>>>(wl[ls[l].rb], dL, l, dS, 1 - (s & 1));
-            n++;
-          }
+          for (int s = 0; s < 3; s++)
+            for (int colour = 0; colour < 2; colour++) {
+              k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour);
+              n++;
+            }
         }
         k_update64<<<go(s_upd), kT, 0, st>>>(wl[s_upd], dJ, dL, dS, kMg);
         k_res64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, kMg, part, nparts);
@@ -893,27 +1018,25 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     for (int j = 0; j < nj; j++) {
       const Lay& Y = lay[j];
       const PbGeom& g = jobs[j].g;
-      long long nint = (long long)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
       if (hs[j].status == kMg) {
         any_mg = true;
         maxlev = std::max(maxlev, Y.nlev);
         for (int l = 0; l < Y.nlev; l++) {
           const PbGeom& a = Y.lv[l];
-          lists.add(ls[l].rb, j,
-                    (long long)((a.nx + kBX - 1) / kBX) * ((a.ny + kBY - 1) / kBY) * ((a.nz + kBZ - 1) / kBZ));
-          lists.add(ls[l].res, j, cdiv((long long)(a.nx - 2) * (a.ny - 2) * (a.nz - 2), kT));
-          lists.add(ls[l].restr, j, cdiv((long long)Y.lv[l + 1].n(), kT));
-          lists.add(ls[l].prol, j, cdiv((long long)a.n(), kT));
+          lists.add(ls[l].rb, j, cdiv((long long)((a.nx - 1) / 2) * (a.ny - 2) * (a.nz - 2), kT));
+          lists.add(ls[l].res, j, nbricks(a));
+          lists.add(ls[l].restr, j, nbricks(Y.lv[l + 1]));
+          lists.add(ls[l].prol, j, nbricks(a));
         }
         lists.add(ls[Y.nlev].coarse, j, 1);
-        lists.add(s_upd, j, cdiv((long long)g.n(), kT));
-        lists.add(s_res, j, cdiv(nint, kT));
+        lists.add(s_upd, j, cdiv(cdiv((long long)g.n(), 4), kT));
+        lists.add(s_res, j, nbricks(g));
         lists.add(s_norm, j, 1);
       } else if (hs[j].status == kSor) {
         any_sor = true;
-        lists.add(s_sres, j, cdiv(nint, kT));
+        lists.add(s_sres, j, nbricks(g));
         lists.add(s_sor, j, cdiv((long long)((g.nx - 1) / 2) * (g.ny - 2) * (g.nz - 2), kT));
-        lists.add(s_supd, j, cdiv((long long)g.n(), kT));
+        lists.add(s_supd, j, cdiv(cdiv((long long)g.n(), 4), kT));
         lists.add(s_snorm, j, 1);
       }
     }
@@ -937,15 +1060,20 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     // grids whose V-cycles diverged continue as SOR from their current
     // potential with the boundary values set again (pb_solver.rs:1118-1125)
     bool switched = false;
+    std::vector<int> redo;
     for (int j = 0; j < nj; j++)
       if (hs[j].status == kDiverged) {
-        pb_boundary(c_, jobs[j].g, hd[j].phi, *jobs[j].atoms, jobs[j].bc);
+        if (jobs[j].bc.kind == 1)
+          redo.push_back(j);
+        else
+          pb_boundary(c_, jobs[j].g, hd[j].phi, *jobs[j].atoms, jobs[j].bc);
         hs[j].status = kSor;
         hs[j].om = 1.0;
         hs[j].sor_it = 0;
         hs[j].rms = DBL_MAX;
         switched = true;
       }
+    dh_launch(redo);
     if (switched) RSTG_CUDA(cudaMemcpyAsync(dS, hs.data(), sizeof(JobState) * nj, cudaMemcpyHostToDevice, st));
     std::vector<int> k2;
     for (int j = 0; j < nj; j++)
