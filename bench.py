@@ -21,6 +21,13 @@ Reported (one JSON line on rank 0):
              bounded sample of the same frames
   serving    p50 / p99 request latency and frames/s of a bounded mixed
              request stream through the serving loop
+  pbsa       MM-PBSA on the 3,000 + 40-atom workload (linearised PB, 0.5 A
+             grid of 145 x 123 x 125 points, Debye-Hueckel boundary, 150 mM):
+             frames/s of the batched mixed-precision engine (FP32 V-cycles
+             under FP64 defect correction) and of the plain FP64 form, the
+             largest polar-term difference between them, per-kernel HBM
+             rooflines of the level-0 multigrid kernels, and the same with the
+             reference's default two-level focusing
 With --gpus N each rank runs its own 1,000 frames (weak scaling, replicas:
 the path has no exchange step).
 """
@@ -119,6 +126,53 @@ def cpu_baseline(s, fr, n_sample):
                       f"C++ restatement of the reference, {O.threads()} OpenMP threads"}
 
 
+PB = dict(grid_spacing=0.5, grid_buffer=12.0, fillratio=0.0)  # linearised PB, DH boundary, no focusing
+
+
+def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs):
+    """MM-PBSA frames/s, batched mixed precision vs plain FP64, same frames."""
+    import torch
+    from rust_simulation_tools import synthetic as S
+
+    s, fr = S.workload(3, n_frames=n_frames)
+    d = tempfile.mkdtemp()
+    S.write_prmtop(s, os.path.join(d, "w3.prmtop"))
+    top = rst.read_prmtop(os.path.join(d, "w3.prmtop"))
+    out = {}
+    for name, kw in (("linear_dh", PB), ("focusing_default", dict(fillratio=4.0))):
+        p = rst.PbParams(**kw)
+        fused = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, pb_params=p, ctx=ctx)
+        fused.run(fr[:2])
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ef = fused.run(fr)
+        tf = time.perf_counter() - t
+        st = fused.pb_stats()
+        plain = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, pb_params=p, mode="plain", ctx=ctx)
+        plain.run(fr[:1])
+        t = time.perf_counter()
+        ep = plain.run(fr[:n_plain])
+        tp = time.perf_counter() - t
+        keys = ("complex_polar", "receptor_polar", "ligand_polar", "delta_polar")
+        err = {k: float(np.abs(ef[:n_plain, c] - ep[:, c]).max()) for k, c in zip(keys, (1, 4, 7, 10))}
+        r = {"fused_frames_per_s": n_frames / tf, "plain_frames_per_s": n_plain / tp,
+             "speedup_vs_plain_gpu": (n_frames / tf) / (n_plain / tp), "frames": n_frames, "plain_frames": n_plain,
+             "max_abs_diff_vs_plain_fp64_kcal": err, "tolerance_kcal": 1e-3,
+             "grids": st["grids"], "lockstep_cycles": st["cycles"], "sor_grids": st["fp64_fallbacks"],
+             "host_ms_setup_cycles_finish": [st["ms_setup"], st["ms_cycles"], st["ms_finish"]]}
+        if name == "linear_dh":  # HBM roofline of the level-0 kernels (event-timed, no graph capture)
+            fused.set_pb_profile(True)
+            fused.run(fr[:8])
+            prof = fused.pb_profile()
+            r["roofline_level0"] = {k: {"achieved_gbs": v["bytes"] / (v["ms"] / 1e3) / 1e9,
+                                        "frac_of_measured_hbm": v["bytes"] / (v["ms"] / 1e3) / 1e9 / peak_gbs,
+                                        "ms": v["ms"], "launches": v["launches"]}
+                                    for k, v in prof.items() if v["ms"] > 0}
+            r["grid"] = "145 x 123 x 125 (complex), 0.5 A, buffer 12 A"
+        out[name] = r
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -193,6 +247,7 @@ def main():
     ap.add_argument("--ref-frames", type=int, default=8)
     ap.add_argument("--plain-frames", type=int, default=16)
     ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--pb-frames", type=int, default=32, help="MM-PBSA leg frames (0: skip)")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e/plain/cpu/serving legs")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -323,6 +378,9 @@ def main():
             extras["cpu_baseline"] = cpu_baseline(s, fr, args.ref_frames)
         if rank == 0 and world == 1 and args.serve_requests > 0:
             extras["serving"] = serving_stream(rst, ctx, args.serve_requests)
+        if rank == 0 and world == 1 and args.pb_frames > 0:
+            peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+            extras["pbsa"] = pbsa_leg(rst, ctx, args.pb_frames, 3, peak)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,

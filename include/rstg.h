@@ -305,6 +305,14 @@ rstg_status rstg_system_last_stats(const rstg_system* s, int64_t* stats4);
 rstg_status rstg_system_pb_stats(const rstg_system* s, double* stats8);
 /* Frames per batched PB launch sequence (0: from the device memory budget). */
 rstg_status rstg_system_set_pb_batch(rstg_system* s, int64_t frames);
+/* Profile mode of the batched PB engine (no reference counterpart): when on,
+ * later runs launch the multigrid cycles without graph capture and time the
+ * level-0 kernels with CUDA events.  rstg_system_pb_profile returns twelve
+ * doubles, for the colour sweep, FP32 residual, FP64 residual and update:
+ * total milliseconds [0..3], algorithmic DRAM bytes of the timed launches
+ * [4..7] and launch counts [8..11], accumulated since profiling began. */
+rstg_status rstg_system_set_pb_profile(rstg_system* s, int32_t on);
+rstg_status rstg_system_pb_profile(const rstg_system* s, double* out12);
 
 /* Per-kernel device time of one pass of the fused engine over device frames
  * (no reference counterpart).  Each kernel is bracketed by CUDA events on the

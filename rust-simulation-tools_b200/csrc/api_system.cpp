@@ -205,6 +205,32 @@ rstg_status rstg_system_pb_stats(const rstg_system* s, double* o) {
   });
 }
 
+rstg_status rstg_system_set_pb_profile(rstg_system* s, int32_t on) {
+  return guard([&] {
+    if (!s) throw Error(RSTG_ERR_INVALID, "system must not be NULL");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    s->pb_profile = on != 0;
+    if (s->pbe) {
+      s->pbe->profile = on != 0;
+      s->pbe->prof = rstg::PbProfile();
+    }
+  });
+}
+
+rstg_status rstg_system_pb_profile(const rstg_system* s, double* o) {
+  return guard([&] {
+    if (!s || !o) throw Error(RSTG_ERR_INVALID, "system and out must not be NULL");
+    for (int k = 0; k < 12; k++) o[k] = 0.0;
+    if (!s->pbe) return;
+    const rstg::PbProfile& p = s->pbe->prof;
+    for (int k = 0; k < rstg::kProfKernels; k++) {
+      o[k] = p.ms[k];
+      o[4 + k] = p.bytes[k];
+      o[8 + k] = (double)p.launches[k];
+    }
+  });
+}
+
 rstg_status rstg_system_set_pb_batch(rstg_system* s, int64_t frames) {
   return guard([&] {
     if (!s) throw Error(RSTG_ERR_INVALID, "system must not be NULL");

@@ -689,6 +689,7 @@ struct Lists {
 
 PbBatchEngine::~PbBatchEngine() {
   if (graph_) cudaGraphExecDestroy(graph_);
+  for (cudaEvent_t e : prof_events_) cudaEventDestroy(e);
 }
 
 void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, const std::vector<double*>* phi_out) {
@@ -937,7 +938,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     }
   }
   const int K = std::max(1, chunk_cycles), KS = 4;  // cycles per chunk, SOR sweeps per cycle
-  bool use_graph = st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+  bool use_graph = !profile && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
   std::vector<int> key;  // (job, status) pairs of the current lists
   std::vector<WL> wl;
   Lists lists;
@@ -949,6 +950,28 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   std::vector<LvSlots> ls(kMaxLev);
   int s_upd = 0, s_res = 0, s_norm = 0, s_sres = 0, s_sor = 0, s_supd = 0, s_snorm = 0, maxlev = 0;
   bool any_mg = false, any_sor = false;
+  // profile mode: events around the level-0 kernels, with their algorithmic
+  // bytes (compulsory DRAM traffic per launch) from the current lists
+  double kbytes[kProfKernels] = {};
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  size_t next_ev = 0;
+  auto mark = [&](int kind, auto&& launch) {
+    if (!profile) {
+      launch();
+      return;
+    }
+    while (prof_events_.size() < 2 * (next_ev + 1)) {
+      cudaEvent_t e;
+      RSTG_CUDA(cudaEventCreate(&e));
+      prof_events_.push_back(e);
+    }
+    cudaEvent_t a = prof_events_[2 * next_ev], b = prof_events_[2 * next_ev + 1];
+    next_ev++;
+    RSTG_CUDA(cudaEventRecord(a, st));
+    launch();
+    RSTG_CUDA(cudaEventRecord(b, st));
+    marks.push_back({kind, {a, b}});
+  };
   auto enqueue_chunk = [&]() {
     int n = 0;
     auto go = [&](int slot) { return lists.slots[slot].total; };
@@ -958,10 +981,16 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           if (go(ls[l].rb)) {
             for (int s = 0; s < 3; s++)
               for (int colour = 0; colour < 2; colour++) {
-                k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour);
+                if (l == 0)
+                  mark(0, [&] { k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour); });
+                else
+                  k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour);
                 n++;
               }
-            k_res32<<<go(ls[l].res), kT, 0, st>>>(wl[ls[l].res], dL, l, dS);
+            if (l == 0)
+              mark(1, [&] { k_res32<<<go(ls[l].res), kT, 0, st>>>(wl[ls[l].res], dL, l, dS); });
+            else
+              k_res32<<<go(ls[l].res), kT, 0, st>>>(wl[ls[l].res], dL, l, dS);
             k_restrict32<<<go(ls[l].restr), kT, 0, st>>>(wl[ls[l].restr], dL, l, dS);
             n += 2;
           }
@@ -976,12 +1005,15 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           n++;
           for (int s = 0; s < 3; s++)
             for (int colour = 0; colour < 2; colour++) {
-              k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour);
+              if (l == 0)
+                mark(0, [&] { k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour); });
+              else
+                k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour);
               n++;
             }
         }
-        k_update64<<<go(s_upd), kT, 0, st>>>(wl[s_upd], dJ, dL, dS, kMg);
-        k_res64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, kMg, part, nparts);
+        mark(3, [&] { k_update64<<<go(s_upd), kT, 0, st>>>(wl[s_upd], dJ, dL, dS, kMg); });
+        mark(2, [&] { k_res64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, kMg, part, nparts); });
         k_norm<<<go(s_norm), 256, 0, st>>>(wl[s_norm], dJ, dS, part, nparts, 1);
         n += 3;
       }
@@ -1040,6 +1072,16 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
         lists.add(s_snorm, j, 1);
       }
     }
+    for (int k = 0; k < kProfKernels; k++) kbytes[k] = 0.0;
+    for (int j = 0; j < nj; j++)
+      if (hs[j].status == kMg) {
+        double pts = (double)jobs[j].g.n();
+        bool u = jobs[j].uniform;
+        kbytes[0] += pts * (u ? 10.0 : 26.0);  // e, rhs, (4 maps), half of e written
+        kbytes[1] += pts * (u ? 12.0 : 28.0);  // e, rhs, (4 maps), res written
+        kbytes[2] += pts * (u ? 20.0 : 52.0);  // phi, rho, (4 FP64 maps), rhs written
+        kbytes[3] += pts * 24.0;               // phi and e read and written
+      }
     lists.upload(lists_, st, wl);
     if (use_graph && (any_mg || any_sor)) {
       cudaGraph_t g = nullptr;
@@ -1096,6 +1138,15 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     stats.cycles += K;
     RSTG_CUDA(cudaMemcpyAsync(hs.data(), dS, sizeof(JobState) * nj, cudaMemcpyDeviceToHost, st));
     RSTG_CUDA(cudaStreamSynchronize(st));
+    for (auto& m : marks) {
+      float t = 0.0f;
+      RSTG_CUDA(cudaEventElapsedTime(&t, m.second.first, m.second.second));
+      prof.ms[m.first] += t;
+      prof.bytes[m.first] += kbytes[m.first];
+      prof.launches[m.first] += 1;
+    }
+    marks.clear();
+    next_ev = 0;
   }
   if (exec) {
     cudaGraphExecDestroy(exec);

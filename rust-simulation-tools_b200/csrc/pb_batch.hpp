@@ -34,6 +34,15 @@ struct PbBatchStats {
   double ms_finish = 0.0;  // FP64 fallbacks, energies
 };
 
+// Per-kernel device time of the level-0 multigrid kernels (profile mode):
+// 0 colour sweep, 1 FP32 residual, 2 FP64 residual, 3 update; bytes are the
+// algorithmic (compulsory) DRAM bytes of the timed launches.
+constexpr int kProfKernels = 4;
+struct PbProfile {
+  double ms[kProfKernels] = {}, bytes[kProfKernels] = {};
+  int64_t launches[kProfKernels] = {};
+};
+
 class PbBatchEngine {
  public:
   PbBatchEngine(Ctx* c, cudaStream_t st) : c_(c), st_(st) {}
@@ -44,6 +53,8 @@ class PbBatchEngine {
   void solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, const std::vector<double*>* phi_out = nullptr);
   void set_stream(cudaStream_t s) { st_ = s; }
   PbBatchStats stats;
+  PbProfile prof;
+  bool profile = false;  // time the level-0 kernels with events (no graph capture)
   int chunk_cycles = 8;  // cycles per graph launch between status reads
 
  private:
@@ -51,6 +62,7 @@ class PbBatchEngine {
   cudaStream_t st_;
   DevBuf pool64_, pool32_, desc_, part_, small_, lists_;
   cudaGraphExec_t graph_ = nullptr;
+  std::vector<cudaEvent_t> prof_events_;
 };
 
 // Polar PB energies (E_solvated - E_reference, pb_energy.rs:332-438) of

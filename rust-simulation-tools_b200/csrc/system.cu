@@ -1311,7 +1311,10 @@ void System::run_pb(const void* frames, bool f64, bool host_in, int64_t F, rstg_
   RSTG_CUDA(cudaMemcpyAsync(res.data(), out, F * sizeof(rstg_frame_energy),
                             host_out ? cudaMemcpyHostToHost : cudaMemcpyDeviceToHost, st));
   RSTG_CUDA(cudaStreamSynchronize(st));
-  if (!pbe) pbe = std::make_unique<PbBatchEngine>(ctx, st);
+  if (!pbe) {
+    pbe = std::make_unique<PbBatchEngine>(ctx, st);
+    pbe->profile = pb_profile;
+  }
   pbe->set_stream(st);
   const Topology* T[3] = {&split.complex, &split.rec, &split.lig};
   const std::vector<int64_t>* sel[3] = {nullptr, &split.rec_atoms, &split.lig_atoms};

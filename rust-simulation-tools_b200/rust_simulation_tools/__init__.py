@@ -739,6 +739,20 @@ class BindingSystem:
         return {"grids": int(st[0]), "cycles": int(st[1]), "fp64_fallbacks": int(st[2]), "ms_setup": st[3],
                 "ms_cycles": st[4], "ms_finish": st[5]}
 
+    def set_pb_profile(self, on: bool = True) -> None:
+        """Time the level-0 PB multigrid kernels with CUDA events on later runs
+        (launches without graph capture while on)."""
+        check(N.lib.rstg_system_set_pb_profile(self._h, int(bool(on))))
+
+    def pb_profile(self) -> dict:
+        """Per-kernel totals of the PB profile mode: ms, algorithmic DRAM bytes
+        and launches of the level-0 colour sweep, FP32 residual, FP64
+        residual and update."""
+        st = np.zeros(12)
+        check(N.lib.rstg_system_pb_profile(self._h, _dp(st)))
+        names = ("sweep", "residual32", "residual64", "update64")
+        return {n: {"ms": st[k], "bytes": st[4 + k], "launches": int(st[8 + k])} for k, n in enumerate(names)}
+
     def set_pb_batch(self, frames: int) -> None:
         """Frames per batched PB launch sequence (0: from the memory budget)."""
         check(N.lib.rstg_system_set_pb_batch(self._h, int(frames)))
