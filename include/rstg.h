@@ -205,6 +205,17 @@ rstg_status rstg_mm_energy_compute(rstg_ctx* ctx, const rstg_topology* t, const 
 rstg_status rstg_gb_energy_compute(rstg_ctx* ctx, const rstg_topology* t, const double* xyz, int64_t n,
                                    const rstg_gb_params* p, double* total, double* born_radii);
 /* compute_sa_energy, crates/mmpbsa/src/sa_energy.rs:51-75 */
+/* Born-radius cache across frames (gb_energy.rs:66-120): when the RMSD
+ * between the coordinates and the cached ones is below rmsd_threshold (A),
+ * compute_gb_energy_cached (gb_energy.rs:372-387) reuses the cached radii;
+ * otherwise it recomputes them and refreshes the cache.  The cache is a host
+ * object; reused (optional) receives 1 on a hit. */
+typedef struct rstg_gb_cache rstg_gb_cache;
+rstg_status rstg_gb_cache_create(double rmsd_threshold, rstg_gb_cache** out);
+void rstg_gb_cache_destroy(rstg_gb_cache* c);
+rstg_status rstg_gb_energy_cached(rstg_ctx* ctx, const rstg_topology* t, const double* xyz, int64_t n,
+                                  const rstg_gb_params* p, rstg_gb_cache* cache, double* total, double* born_radii,
+                                  int32_t* reused);
 rstg_status rstg_sa_energy_compute(rstg_ctx* ctx, const rstg_topology* t, const double* xyz, int64_t n,
                                    const rstg_sa_params* p, double* total, double* total_sasa, double* per_atom);
 /* compute_pb_energy / compute_pb_energy_solvated, crates/mmpbsa/src/pb_energy.rs:332-482;

@@ -86,6 +86,8 @@ def lib():
         L.orc_kappa.argtypes = [C.c_double] * 3
         L.orc_gb_energy.restype = C.c_double
         L.orc_gb_energy.argtypes = [vp, dp, C.POINTER(GbP), C.c_int, dp]
+        L.orc_gb_energy_from_radii.restype = C.c_double
+        L.orc_gb_energy_from_radii.argtypes = [vp, dp, C.POINTER(GbP), dp]
         L.orc_mm_energy.argtypes = [vp, dp, C.c_int, dp]
         L.orc_sa_energy.restype = C.c_double
         L.orc_sa_energy.argtypes = [vp, dp, C.POINTER(SaP), dp, dp]
@@ -240,6 +242,12 @@ def gb_energy(top: Topology, xyz_A, params: GbP = None, accurate=False):
     R = np.zeros(top.n_atoms)
     e = lib().orc_gb_energy(top.h, _d(x), C.byref(params or gb_params()), int(accurate), _d(R))
     return e, R
+
+
+def gb_energy_from_radii(top: Topology, xyz_A, params: GbP, radii) -> float:
+    x = np.ascontiguousarray(xyz_A, dtype=np.float64)
+    r = np.ascontiguousarray(radii, dtype=np.float64)
+    return lib().orc_gb_energy_from_radii(top.h, _d(x), C.byref(params), _d(r))
 
 
 def mm_energy(top: Topology, xyz_A, accurate=False) -> np.ndarray:

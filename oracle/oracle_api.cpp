@@ -589,6 +589,15 @@ double orc_gb_energy(void* h, const double* xyz_A, const orc_gb_params* p, int a
   return gb_energy_from_radii(*t, x, g, R, accurate != 0);
 }
 
+// compute_gb_energy_from_radii with given radii (gb_energy.rs:283-355), the
+// energy compute_gb_energy_cached returns on a cache hit (gb_energy.rs:372-387).
+double orc_gb_energy_from_radii(void* h, const double* xyz_A, const orc_gb_params* p, const double* radii) {
+  Topology* t = T(h);
+  auto x = coords(xyz_A, t->n_atoms);
+  std::vector<double> r(radii, radii + t->n_atoms);
+  return gb_energy_from_radii(*t, x, gbp(p), r, false);
+}
+
 void orc_mm_energy(void* h, const double* xyz_A, int accurate, double* out7) {
   Topology* t = T(h);
   MmEnergy e = mm_energy(*t, coords(xyz_A, t->n_atoms), accurate != 0);

@@ -445,6 +445,76 @@ rstg_status rstg_gb_energy_compute(rstg_ctx* c, const rstg_topology* t, const do
   });
 }
 
+}  // extern "C"
+
+struct rstg_gb_cache {
+  std::vector<double> coords, radii;
+  double threshold = 0.5;
+};
+
+extern "C" {
+
+rstg_status rstg_gb_cache_create(double rmsd_threshold, rstg_gb_cache** out) {
+  return guard([&] {
+    need(out, "out");
+    auto c = std::make_unique<rstg_gb_cache>();
+    c->threshold = rmsd_threshold;
+    *out = c.release();
+  });
+}
+
+void rstg_gb_cache_destroy(rstg_gb_cache* c) { delete c; }
+
+rstg_status rstg_gb_energy_cached(rstg_ctx* c, const rstg_topology* t, const double* xyz, int64_t n,
+                                  const rstg_gb_params* p, rstg_gb_cache* cache, double* total, double* born,
+                                  int32_t* reused) {
+  return guard([&] {
+    need(c, "ctx");
+    need(cache, "cache");
+    need(total, "total");
+    check_coords(t, xyz, n);
+    rstg_gb_params gp;
+    if (p)
+      gp = *p;
+    else
+      rstg_gb_params_default(&gp);
+    check_gb(gp);
+    // try_reuse (gb_energy.rs:88-110): same atom count, RMSD summed in atom order
+    bool hit = false;
+    if (n > 0 && (int64_t)cache->coords.size() == 3 * n) {
+      double sum_sq = 0.0;
+      for (int64_t a = 0; a < n; a++) {
+        double dx = cache->coords[3 * a] - xyz[3 * a], dy = cache->coords[3 * a + 1] - xyz[3 * a + 1],
+               dz = cache->coords[3 * a + 2] - xyz[3 * a + 2];
+        sum_sq += dx * dx + dy * dy + dz * dz;
+      }
+      hit = std::sqrt(sum_sq / (double)n) < cache->threshold;
+    }
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    c->bind();
+    OneShot o(c, *t, xyz);
+    DevBuf R(std::max<int64_t>(n, 1) * 8, c->stream), e(8, c->stream);
+    RSTG_CUDA(cudaMemsetAsync(e.p, 0, 8, c->stream));
+    if (n) {
+      if (hit)
+        RSTG_CUDA(cudaMemcpyAsync(R.p, cache->radii.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+      else
+        plain_born_radii(c, o.dev, o.xyz.as<double>(), gp, R.as<double>());
+      plain_gb_energy(c, o.dev, o.xyz.as<double>(), gp, R.as<double>(), e.as<double>());
+    }
+    std::vector<double> hr(n);
+    RSTG_CUDA(cudaMemcpyAsync(total, e.p, 8, cudaMemcpyDeviceToHost, c->stream));
+    if (n) RSTG_CUDA(cudaMemcpyAsync(hr.data(), R.p, n * 8, cudaMemcpyDeviceToHost, c->stream));
+    RSTG_CUDA(cudaStreamSynchronize(c->stream));
+    if (!hit) {  // update (gb_energy.rs:112-119)
+      cache->coords.assign(xyz, xyz + 3 * n);
+      cache->radii = hr;
+    }
+    if (born && n) memcpy(born, hr.data(), n * 8);
+    if (reused) *reused = hit ? 1 : 0;
+  });
+}
+
 rstg_status rstg_sa_energy_compute(rstg_ctx* c, const rstg_topology* t, const double* xyz, int64_t n,
                                    const rstg_sa_params* p, double* total, double* total_sasa, double* per_atom) {
   return guard([&] {

@@ -28,7 +28,7 @@ __all__ = [
     "DecompositionResult", "EntropyEstimate", "compute_mm_energy", "compute_gb_energy", "compute_sa_energy",
     "compute_pb_energy", "compute_binding_energy", "compute_binding_energy_single_frame",
     "decompose_binding_energy", "interaction_entropy", "quasi_harmonic_entropy", "extract_subtopology",
-    "BindingSystem", "Server", "device_count", "kernel_launches",
+    "BindingSystem", "Server", "device_count", "kernel_launches", "GbCache", "compute_gb_energy_cached",
 ]
 
 USIZE_MAX = 2 ** 64 - 1
@@ -543,6 +543,41 @@ def compute_gb_energy(topology: AmberTopology, coords, gb_params: GbParams = Non
     R = np.zeros(len(x))
     check(N.lib.rstg_gb_energy_compute(N.ctx(), topology._h, _dp(x), len(x), C.byref(_gb(gb_params)),
                                        C.byref(tot), _dp(R)))
+    return GbEnergy(tot.value, R)
+
+
+class GbCache:
+    """Born radii kept from a previous frame (gb_energy.rs:66-120): a frame
+    whose RMSD to the cached coordinates is below ``rmsd_threshold`` (A)
+    reuses them.  Rust-crate API; the reference's Python module does not
+    expose it."""
+
+    def __init__(self, rmsd_threshold: float = 0.5):
+        h = N.vp()
+        check(N.lib.rstg_gb_cache_create(float(rmsd_threshold), C.byref(h)))
+        self._h = h
+        self.last_reused = False
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib.rstg_gb_cache_destroy(h)
+            self._h = None
+
+
+def compute_gb_energy_cached(topology: AmberTopology, coords, gb_params: GbParams = None,
+                             cache: GbCache = None) -> GbEnergy:
+    """compute_gb_energy_cached (gb_energy.rs:372-387); coords in nm like the
+    other calls.  ``cache.last_reused`` tells whether the radii were reused."""
+    if cache is None:
+        raise ValueError("cache must be a GbCache")
+    x = _coords_A(coords)
+    tot = C.c_double()
+    R = np.zeros(len(x))
+    hit = C.c_int32()
+    check(N.lib.rstg_gb_energy_cached(N.ctx(), topology._h, _dp(x), len(x), C.byref(_gb(gb_params)), cache._h,
+                                      C.byref(tot), _dp(R), C.byref(hit)))
+    cache.last_reused = bool(hit.value)
     return GbEnergy(tot.value, R)
 
 

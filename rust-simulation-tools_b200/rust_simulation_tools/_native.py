@@ -123,6 +123,9 @@ _sig("rstg_dcd_read_f32", C.c_int, cs, fp, i64, ip, ip)
 _sig("rstg_mdcrd_read", C.c_int, cs, i64, i32, dp, i64, ip)
 _sig("rstg_mm_energy_compute", C.c_int, vp, vp, dp, i64, P(MmEnergy))
 _sig("rstg_gb_energy_compute", C.c_int, vp, vp, dp, i64, P(GbParams), dp, dp)
+_sig("rstg_gb_cache_create", C.c_int, dbl, P(vp))
+_sig("rstg_gb_cache_destroy", None, vp)
+_sig("rstg_gb_energy_cached", C.c_int, vp, vp, dp, i64, P(GbParams), vp, dp, dp, P(i32))
 _sig("rstg_sa_energy_compute", C.c_int, vp, vp, dp, i64, P(SaParams), dp, dp, dp)
 _sig("rstg_pb_energy_compute", C.c_int, vp, vp, dp, i64, P(PbParams), ip, i64, dp, P(PbDiag))
 _sig("rstg_pb_grid_maps", C.c_int, vp, dp, i64, dp, dp, P(PbParams), dbl, dbl, i32, ip, dp, dp, P(C.c_uint8), dp, dp,

@@ -311,3 +311,58 @@ def test_server_results_same_alone_and_in_mix(rst, sysdata):
     st = srv.stats()
     assert st["completed"] == 4 and st["p99_ms"] >= st["p50_ms"] > 0
     srv.close()
+
+
+def test_gb_cache_reuses_radii(rst, oracle, sysdata):
+    # gb_energy.rs:66-120,372-387: first call computes and caches the radii;
+    # a frame within the RMSD threshold reuses them (energy from the cached
+    # radii at the new coordinates); a frame beyond it recomputes.
+    s, fr, prm, _ = sysdata
+    top, otop = rst.read_prmtop(prm), oracle.Topology.load(prm)
+    gp = rst.GbParams(model=2)
+    og = oracle.gb_params("obc2")
+    x0 = dcd_coords(fr[0])
+    cache = rst.GbCache(0.5)
+    a = rst.compute_gb_energy_cached(top, x0 / 10.0, gp, cache)
+    assert not cache.last_reused
+    b = rst.compute_gb_energy(top, x0 / 10.0, gp)
+    assert a.total == b.total
+    np.testing.assert_array_equal(a.born_radii(), b.born_radii())
+    x1 = x0 + 0.05  # RMSD 0.087 A
+    c = rst.compute_gb_energy_cached(top, x1 / 10.0, gp, cache)
+    assert cache.last_reused
+    np.testing.assert_array_equal(c.born_radii(), a.born_radii())
+    ref = oracle.gb_energy_from_radii(otop, (x1 / 10.0) * 10.0, og, a.born_radii())
+    assert rel(c.total, ref) < 1e-10
+    x2 = dcd_coords(fr[1])  # sigma 0.5 A noise per coordinate: RMSD ~1.2 A
+    d = rst.compute_gb_energy_cached(top, x2 / 10.0, gp, cache)
+    assert not cache.last_reused
+    assert d.total == rst.compute_gb_energy(top, x2 / 10.0, gp).total
+
+
+def test_sharded_frames_equal_single_process(rst, sysdata):
+    import datetime
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from rust_simulation_tools import sharding as SH
+
+    s, fr, prm, _ = sysdata
+    top = rst.read_prmtop(prm)
+    sysf = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues)
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        rows = SH.binding_frames_sharded(sysf, fr)
+    finally:
+        dist.destroy_process_group()
+    np.testing.assert_array_equal(rows, sysf.run(fr))
+    st = SH.statistics(rows)
+    d = rows[:, 12]
+    assert abs(st["mean_delta_total"] - d.mean()) < 1e-9 and abs(st["std_delta_total"] - d.std(ddof=1)) < 1e-9
