@@ -32,6 +32,7 @@ With --gpus N each rank runs its own 1,000 frames (weak scaling, replicas:
 the path has no exchange step).
 """
 import argparse
+import faulthandler
 import json
 import os
 import subprocess
@@ -196,9 +197,20 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _fifo_latencies(arrivals, service):
+    """Latencies of requests served one at a time in arrival order."""
+    t, lat = 0.0, []
+    for a, sv in zip(arrivals, service):
+        t = max(t, a) + sv
+        lat.append(t - a)
+    return np.array(lat)
+
+
 def serving_stream(rst, ctx, n_req, seed=4):
     """Bounded mixed stream: receptors log-uniform 1k-20k atoms, ligands
-    20-80 atoms, 1-200 frames per request, Poisson arrivals."""
+    20-80 atoms, 1-200 frames per request, Poisson arrivals; beside it the
+    same requests one at a time (fused engine, and plain FP64 form from its
+    per-frame time on each system) on the same arrival times."""
     from rust_simulation_tools import synthetic as S
 
     rng = np.random.default_rng(seed)
@@ -211,21 +223,25 @@ def serving_stream(rst, ctx, n_req, seed=4):
         p = os.path.join(d, f"s{k}.prmtop")
         S.write_prmtop(s, p)
         top = rst.read_prmtop(p)
-        bs = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, gb_params=rst.GbParams(**GB),
-                               sa_params=rst.SaParams(n_sphere_points=NPTS), ctx=ctx)
-        systems.append((s, bs))
+        kw = dict(gb_params=rst.GbParams(**GB), sa_params=rst.SaParams(n_sphere_points=NPTS), ctx=ctx)
+        bs = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, **kw)
+        bp = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, mode="plain", **kw)
+        systems.append((s, bs, bp, nr))
     reqs = []
     for _ in range(n_req):
         k = int(rng.integers(0, len(systems)))
         reqs.append((k, S.make_frames(systems[k][0], int(rng.integers(1, 201)), seed=int(rng.integers(1 << 30)))))
-    for k, (s, bs) in enumerate(systems):  # first-use preparation outside the stream
+    for s, bs, bp, _ in systems:  # first-use preparation outside the stream
         bs.run(S.make_frames(s, 1, seed=1))
     srv = rst.Server(max_inflight=4, ctx=ctx)
     gaps = rng.exponential(0.01, size=n_req)
+    arrivals = np.cumsum(gaps)
     t0 = time.perf_counter()
     ids = []
-    for (k, fr), g in zip(reqs, gaps):
-        time.sleep(g)
+    for (k, fr), a in zip(reqs, arrivals):
+        dt = a - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
         ids.append(srv.submit(systems[k][1], fr))
     for i in ids:
         srv.wait(i, 600000)
@@ -233,11 +249,84 @@ def serving_stream(rst, ctx, n_req, seed=4):
     st = srv.stats()
     srv.close()
     frames = sum(fr.shape[0] for _, fr in reqs)
-    return {"requests": n_req, "frames": frames, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "frames_per_s": frames / wall, "arrival_mean_ms": 10.0}
+    # one request at a time through the fused engine (measured service times)
+    svc = []
+    for k, fr in reqs:
+        t = time.perf_counter()
+        systems[k][1].run(fr)
+        svc.append(time.perf_counter() - t)
+    lat = _fifo_latencies(arrivals, svc)
+    # plain FP64 form: per-frame time of each system on 2 frames
+    per_frame = []
+    for s, bs, bp, _ in systems:
+        f2 = S.make_frames(s, 3, seed=2)
+        bp.run(f2[:1])
+        t = time.perf_counter()
+        bp.run(f2[1:])
+        per_frame.append((time.perf_counter() - t) / 2)
+    psvc = [per_frame[k] * fr.shape[0] for k, fr in reqs]
+    plat = _fifo_latencies(arrivals, psvc)
+    return {"requests": n_req, "frames": frames, "receptor_atoms": [int(x[3]) for x in systems],
+            "continuous_batching": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "frames_per_s": frames / wall},
+            "one_at_a_time_fused": {"p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                                    "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                                    "frames_per_s": frames / sum(svc)},
+            "one_at_a_time_plain_fp64": {"p50_ms": 1e3 * float(np.percentile(plat, 50)),
+                                         "p99_ms": 1e3 * float(np.percentile(plat, 99)),
+                                         "frames_per_s": frames / sum(psvc),
+                                         "how": "per-frame time of each system measured on 2 frames; FIFO queue "
+                                                "on the same arrival times"},
+            "arrival_mean_ms": 10.0}
+
+
+def large_mixed(rst, ctx, gb_requests=6, gb_frames=24, pb_requests=2, pb_frames=2, seed=5):
+    """Bounded large mixed load: 25,000 + 80 atoms, MM-GBSA (SASA 960 points)
+    and MM-PBSA (0.5 A grids of ~193^3, DH boundary) requests interleaved in
+    one serving loop; errors against the plain FP64 form on one frame."""
+    from rust_simulation_tools import synthetic as S
+
+    s, fr = S.workload(5, n_frames=max(gb_frames, pb_frames) + 1)
+    d = tempfile.mkdtemp()
+    S.write_prmtop(s, os.path.join(d, "w5.prmtop"))
+    top = rst.read_prmtop(os.path.join(d, "w5.prmtop"))
+    gbkw = dict(gb_params=rst.GbParams(**GB), sa_params=rst.SaParams(n_sphere_points=NPTS), ctx=ctx)
+    pbp = rst.PbParams(grid_spacing=0.5, grid_buffer=11.2, fillratio=0.0)
+    pbkw = dict(pb_params=pbp, sa_params=rst.SaParams(n_sphere_points=NPTS), ctx=ctx)
+    gsys = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, **gbkw)
+    psys = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, **pbkw)
+    gsys.run(fr[:1])
+    psys.run(fr[:1])
+    rng = np.random.default_rng(seed)
+    kinds = ["gb"] * gb_requests + ["pb"] * pb_requests
+    rng.shuffle(kinds)
+    srv = rst.Server(max_inflight=4, ctx=ctx)
+    t0 = time.perf_counter()
+    ids = []
+    for k in kinds:
+        time.sleep(float(rng.exponential(0.02)))
+        ids.append((k, srv.submit(gsys if k == "gb" else psys, fr[1:1 + (gb_frames if k == "gb" else pb_frames)])))
+    outs = [(k, srv.wait(i, 1200000)) for k, i in ids]
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    frames = sum(o.shape[0] for _, o in outs)
+    err = {}
+    for k, sysk in (("gb", rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, mode="plain", **gbkw)),
+                    ("pb", rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, mode="plain", **pbkw))):
+        ref = sysk.run(fr[1:2])
+        got = next(o for kk, o in outs if kk == k)[:1]
+        err[k] = {"delta_polar": float(abs(got[0, 10] - ref[0, 10])), "delta_sa": float(abs(got[0, 11] - ref[0, 11])),
+                  "complex_polar": float(abs(got[0, 1] - ref[0, 1]))}
+    return {"atoms": int(s.n_atoms if hasattr(s, "n_atoms") else 25080), "gb_requests": gb_requests,
+            "gb_frames_per_request": gb_frames, "pb_requests": pb_requests, "pb_frames_per_request": pb_frames,
+            "frames": frames, "frames_per_s": frames / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "pb_stats": psys.pb_stats(), "abs_diff_vs_plain_fp64_frame1_kcal": err,
+            "note": "delta_mm of the plain form carries the reference's cancellation (see DESIGN); polar and SA "
+                    "terms compared"}
 
 
 def main():
+    faulthandler.enable()  # a crash in native code prints the Python stack
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -248,6 +337,7 @@ def main():
     ap.add_argument("--plain-frames", type=int, default=16)
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--pb-frames", type=int, default=32, help="MM-PBSA leg frames (0: skip)")
+    ap.add_argument("--no-large", action="store_true", help="skip the 25,080-atom mixed GB/PB serving leg")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e/plain/cpu/serving legs")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -381,6 +471,8 @@ def main():
         if rank == 0 and world == 1 and args.pb_frames > 0:
             peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
             extras["pbsa"] = pbsa_leg(rst, ctx, args.pb_frames, 3, peak)
+        if rank == 0 and world == 1 and not args.no_large:
+            extras["large_mixed"] = large_mixed(rst, ctx)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,

@@ -52,10 +52,42 @@ struct Server {
 
   Server(Ctx* c, const rstg_server_opts& o) : ctx(c), opts(o) {
     int n = std::max(1, opts.max_inflight);
-    streams.resize(n);
     c->bind();
-    for (int k = 0; k < n; k++) RSTG_CUDA(cudaStreamCreateWithFlags(&streams[k], cudaStreamNonBlocking));
+    streams = take_streams(c->device, n);
     for (int k = 0; k < n; k++) slots.emplace_back([this, k] { slot_loop(k); });
+  }
+
+  // Slot streams come from a per-device pool and are never destroyed: a
+  // system that grew device buffers during a request frees them later with
+  // cudaFreeAsync on the stream they were allocated on, which must still
+  // exist then, whenever the system is destroyed.
+  static std::mutex& pool_mu() {
+    static std::mutex m;
+    return m;
+  }
+  static std::map<int, std::vector<cudaStream_t>>& pool() {
+    static auto* p = new std::map<int, std::vector<cudaStream_t>>();
+    return *p;
+  }
+  static std::vector<cudaStream_t> take_streams(int device, int n) {
+    std::lock_guard<std::mutex> lk(pool_mu());
+    std::vector<cudaStream_t>& free = pool()[device];
+    std::vector<cudaStream_t> out;
+    while ((int)out.size() < n && !free.empty()) {
+      out.push_back(free.back());
+      free.pop_back();
+    }
+    while ((int)out.size() < n) {
+      cudaStream_t s;
+      RSTG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      out.push_back(s);
+    }
+    return out;
+  }
+  static void give_streams(int device, const std::vector<cudaStream_t>& s) {
+    std::lock_guard<std::mutex> lk(pool_mu());
+    auto& free = pool()[device];
+    free.insert(free.end(), s.begin(), s.end());
   }
 
   ~Server() {
@@ -66,10 +98,8 @@ struct Server {
     cv_work.notify_all();
     for (auto& t : slots) t.join();
     ctx->bind();
-    for (auto s : streams) {
-      cudaStreamSynchronize(s);
-      cudaStreamDestroy(s);
-    }
+    for (auto s : streams) cudaStreamSynchronize(s);
+    give_streams(ctx->device, streams);
   }
 
   // Next admissible request: first in arrival order whose system is idle and

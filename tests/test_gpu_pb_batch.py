@@ -104,3 +104,43 @@ def test_pb_fused_frame_alone_equals_batch(rst, small):
     one.set_pb_batch(1)
     b = np.concatenate([one.run(fr[f:f + 1]) for f in range(len(fr))])
     np.testing.assert_array_equal(a, b)
+
+
+def test_server_mixes_pb_and_gb_requests(rst, small):
+    # PB and GB requests interleaved in one serving loop: each result is the
+    # same bits as the request run alone
+    s, fr, prm = small
+    top = rst.read_prmtop(prm)
+    pbs = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues,
+                            pb_params=rst.PbParams(grid_spacing=0.6, grid_buffer=4.0, fillratio=4.0))
+    gbs = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues)
+    alone_p, alone_g = pbs.run(fr), gbs.run(fr)
+    srv = rst.Server(max_inflight=3)
+    ids = [srv.submit(pbs, fr), srv.submit(gbs, fr), srv.submit(pbs, fr[1:]), srv.submit(gbs, fr[:2])]
+    res = [srv.wait(i, 600000) for i in ids]
+    st = srv.stats()
+    srv.close()
+    np.testing.assert_array_equal(res[0], alone_p)
+    np.testing.assert_array_equal(res[1], alone_g)
+    np.testing.assert_array_equal(res[2], alone_p[1:])
+    np.testing.assert_array_equal(res[3], alone_g[:2])
+    assert st["completed"] == 4
+
+
+def test_system_outlives_server_after_growing_buffers(rst, small):
+    # buffers a system allocates while a server runs its request belong to a
+    # server slot stream; destroying the system after the server must be safe
+    import gc
+
+    s, fr, prm = small
+    top = rst.read_prmtop(prm)
+    for kw in (dict(pb_params=rst.PbParams(grid_spacing=0.6, grid_buffer=4.0)), {}):
+        sysx = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, **kw)
+        one = sysx.run(fr[:1])
+        srv = rst.Server(max_inflight=2)
+        rid = srv.submit(sysx, fr)  # three frames: per-batch buffers grow on the slot stream
+        got = srv.wait(rid, 600000)
+        srv.close()
+        np.testing.assert_array_equal(got[:1], one)
+        del sysx, srv
+        gc.collect()
