@@ -153,7 +153,8 @@ __global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __r
                                                const double* __restrict__ rad64, const double* __restrict__ q64,
                                                GbConstF k, float probe, int cap, int* __restrict__ nbr,
                                                int* __restrict__ nbrcnt, double* __restrict__ R64,
-                                               float4* __restrict__ Rf, double* __restrict__ part,
+                                               float4* __restrict__ Rf, float* __restrict__ dRf,
+                                               double* __restrict__ part,
                                                int* __restrict__ diag) {
   __shared__ float4 sx[kTile];
   __shared__ float2 sp[kTile];
@@ -232,6 +233,7 @@ __global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __r
     R64[2 * o] = Rc;
     R64[2 * o + 1] = Rs;
     Rf[o] = make_float4((float)Rc, (float)Rs, (float)(1.0 / Rc), (float)(1.0 / Rs));
+    dRf[o] = (float)(Rc - Rs);
     double q = q64[i], ec = self64(q, Rc, k), es = self64(q, Rs, k);
     sC = ec;
     sD = ec - es;
@@ -257,14 +259,60 @@ __global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __r
 // ---------------------------------------------------------------------------
 // K2: pair energies on triangular tiles
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float gb_pair32(float qq, float r2, float RiRj, float t, const GbConstF& k) {
-  // f_GB = sqrt(r2 + RiRj exp(-r2 / (4 RiRj))) (gb_energy.rs:339-346); t = r2 / (4 RiRj)
-  float e = t < 16.f ? __expf(-t) : 0.f;
-  float f2 = fmaf(RiRj, e, r2);
-  float finv = rsqrtf(f2);
-  if (k.no_salt) return k.fdns * qq * finv;
+// GB pair energy (gb_energy.rs:339-353) with its ingredients:
+// f_GB^2 = r2 + RiRj e, e = exp(-t), t = r2 / (4 RiRj); E = exp(-0.73 kappa f).
+__device__ __forceinline__ float gb_pair_parts(float qq, float r2, float RiRj, float t, const GbConstF& k, float& e,
+                                               float& f2, float& finv, float& E) {
+  e = t < 16.f ? __expf(-t) : 0.f;
+  f2 = fmaf(RiRj, e, r2);
+  finv = rsqrtf(f2);
+  if (k.no_salt) {
+    E = 0.f;
+    return k.fdns * qq * finv;
+  }
   float f = f2 * finv;
-  return -0.5f * qq * (k.fie - __expf(-k.fk * f) * k.fio) * finv;
+  E = __expf(-k.fk * f);
+  return -0.5f * qq * (k.fie - E * k.fio) * finv;
+}
+
+__device__ __forceinline__ float gb_pair32(float qq, float r2, float RiRj, float t, const GbConstF& k) {
+  float e, f2, finv, E;
+  return gb_pair_parts(qq, r2, RiRj, t, k, e, f2, finv, E);
+}
+
+// exp(x) - 1 without cancellation for |x| < 0.2: Taylor to x^6 (relative
+// error below x^6 / 5040 < 1.3e-8), and to x^4 where |x| < 0.1 is known
+// (relative error below x^4 / 120 < 1e-6 of a term that is itself a small
+// correction).
+__device__ __forceinline__ float expm1_6(float x) {
+  return x * (1.f + x * (0.5f + x * (1.f / 6.f + x * (1.f / 24.f + x * (1.f / 120.f + x * (1.f / 720.f))))));
+}
+__device__ __forceinline__ float expm1_4(float x) { return x * (1.f + x * (0.5f + x * (1.f / 6.f + x * (1.f / 24.f)))); }
+
+// p(complex radii) - p(subsystem radii) of one pair, evaluated from the
+// differences themselves so that its rounding is relative to the difference,
+// not to p: dRR = RcRc' - RsRs' comes from the FP64 radius differences;
+// exp(-tS) = exp(-tC) (1 + expm1(tC - tS)) with tC - tS = -tC dRR / RRs;
+// 1/fC - 1/fS = -(fC - fS)/(fC fS); E/f likewise through expm1.  eC, f2C,
+// finvC, EC are the complex pair's ingredients, iRRs = 1 / RRs.
+__device__ __forceinline__ float gb_pair_delta(float qq, float r2, float RRc, float RRs, float iRRs, float dRR,
+                                               float tC, float tS, float eC, float f2C, float finvC, float EC,
+                                               const GbConstF& k) {
+  float dt = -tC * dRR * iRRs;  // tC - tS
+  float g;                      // RRc eC - RRs eS
+  if (fabsf(dt) < 0.2f && tC < 16.f) {
+    g = eC * (dRR - RRs * expm1_6(dt));
+  } else {
+    float eS = tS < 16.f ? __expf(-tS) : 0.f;
+    g = RRc * eC - RRs * eS;
+  }
+  float f2S = f2C - g;
+  float finvS = rsqrtf(f2S);
+  float df = __fdividef(g, f2C * finvC + f2S * finvS);  // fC - fS
+  float dinv = -df * finvC * finvS;                     // 1/fC - 1/fS
+  if (k.no_salt) return k.fdns * qq * dinv;
+  float dh = EC * (dinv - expm1_4(k.fk * df) * finvS);  // EC/fC - ES/fS
+  return -0.5f * qq * (k.fie * dinv - k.fio * dh);
 }
 
 __device__ __forceinline__ double nb64(const double* X64, int i, int j, double qq, double A, double B, int cls,
@@ -281,13 +329,15 @@ struct PairOut {
 
 __global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __restrict__ tiles,
                                                  const float4* __restrict__ xyz32, const double* __restrict__ xyz64,
-                                                 const float4* __restrict__ Rf, const int* __restrict__ type, int nt,
+                                                 const float4* __restrict__ Rf, const float* __restrict__ dRf,
+                                                 const int* __restrict__ type, int nt,
                                                  const float2* __restrict__ lj32, const double2* __restrict__ lj64,
                                                  const unsigned* __restrict__ masks, GbConstF k, double scee,
                                                  double scnb, double* __restrict__ part, int* __restrict__ diag) {
   extern __shared__ float2 slj[];  // nt*nt (A, B)
   __shared__ float4 sx[kTile];
   __shared__ float4 sR[kTile];
+  __shared__ float sdR[kTile];
   __shared__ int st[kTile];
   __shared__ double sh[32];
   for (int t = threadIdx.x; t < nt * nt; t += blockDim.x) slj[t] = lj32[t];
@@ -297,10 +347,12 @@ __global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __r
   const float4* X = xyz32 + (long long)f * nC;
   const double* X64 = xyz64 + (long long)f * nC * 3;
   const float4* RF = Rf + (long long)f * nC;
+  const float* DR = dRf + (long long)f * nC;
   int jl = j0 + threadIdx.x;
   if (jl < nC) {
     sx[threadIdx.x] = X[jl];
     sR[threadIdx.x] = RF[jl];
+    sdR[threadIdx.x] = DR[jl];
     st[threadIdx.x] = type[jl];
   }
   __syncthreads();
@@ -309,6 +361,7 @@ __global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __r
   if (i < nC) {
     float4 xi = X[i];
     float4 Ri = RF[i];
+    float dRi = DR[i];
     int ti = type[i];
     bool in_r = i < nR;
     float iRc = Ri.z, iRs = Ri.w;
@@ -336,14 +389,20 @@ __global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __r
         bool same = (j < nR) == in_r;
         float iRcj = Rj.z;
         float tc = 0.25f * r2 * iRc * iRcj;
-        float pC = gb_pair32(qq, r2, Ri.x * Rj.x, tc, k);
+        float RRc = Ri.x * Rj.x;
+        float eC, f2C, finvC, EC;
+        float pC = gb_pair_parts(qq, r2, RRc, tc, k, eC, f2C, finvC, EC);
         a[0] += pC;
         if (same) {
           float iRsj = Rj.w;
           float ts = 0.25f * r2 * iRs * iRsj;
-          float pS = (tc >= 16.f && ts >= 16.f) ? pC : gb_pair32(qq, r2, Ri.y * Rj.y, ts, k);
-          a[in_r ? 1 : 2] += pS;
-          a[3] += pC - pS;
+          float dRR = fmaf(Ri.x, sdR[jj], Rj.y * dRi);  // RcRc' - RsRs'
+          float iRRs = iRs * iRsj;
+          float dp = (dRR == 0.f || (tc >= 16.f && ts >= 16.f))
+                         ? 0.f
+                         : gb_pair_delta(qq, r2, RRc, Ri.y * Rj.y, iRRs, dRR, tc, ts, eC, f2C, finvC, EC, k);
+          a[in_r ? 1 : 2] += pC - dp;
+          a[3] += dp;
           int cls = 1;
           if (rec >= 0) {
             int w = jj >> 5, b = jj & 31;
@@ -365,9 +424,7 @@ __global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __r
               a[in_r ? 4 : 5] += fmaf(ab.x * ir6, ir6, fmaf(-ab.y, ir6, qq * rinv));
             }
           }
-        } else {
-          a[3] += pC;
-        }
+        }  // receptor x ligand GB pairs enter the binding difference in FP64 (k_rl_rows)
       }
       for (int q = 0; q < 6; q++) acc[q] += (double)a[q];
     }
@@ -546,23 +603,39 @@ __device__ __forceinline__ void rl_pair(const double* X64, const double* q64, co
   }
 }
 
+// GB pair energy in FP64 with the reference's expression (gb_energy.rs:339-353).
+__device__ __forceinline__ double gb_pair64(double qq, double r2, double RR, const GbConstF& k) {
+  double f = sqrt(r2 + RR * exp(-r2 / (4.0 * RR)));
+  if (k.no_salt) return k.diel_ns * qq / f;
+  return -0.5 * qq * (k.inv_ein - exp(-kKScale * k.kappa * f) * k.inv_eout) / f;
+}
+
+// rows [nR][3]: vdw, elec and GB pair sums of each receptor atom over the
+// ligand atoms; the GB sum (complex radii) is the cross part of the binding
+// GB difference, kept in FP64 because each such pair enters it whole.
 __global__ void k_rl_rows(int nC, int nR, const double* __restrict__ xyz64, const double* __restrict__ q64,
                           const int* __restrict__ type, int nt, const double2* __restrict__ lj64,
                           const int* __restrict__ tile_rec, int nb, const unsigned* __restrict__ masks, double scee,
-                          double scnb, double* __restrict__ rows) {
+                          double scnb, const double* __restrict__ R64, GbConstF k, double* __restrict__ rows) {
   int a = blockIdx.x * blockDim.x + threadIdx.x, f = blockIdx.y;
   if (a >= nR) return;
   const double* X64 = xyz64 + (long long)f * nC * 3;
-  double sv = 0.0, se = 0.0;
+  const double* RC = R64 + (long long)f * nC * 2;
+  double sv = 0.0, se = 0.0, sg = 0.0;
+  double Ra = RC[2 * a], qa = q64[a];
   for (int b = nR; b < nC; b++) {
     double v, e;
     rl_pair(X64, q64, type, nt, lj64, tile_rec, nb, masks, scee, scnb, a, b, v, e);
     sv += v;
     se += e;
+    double dx = X64[3 * a] - X64[3 * b], dy = X64[3 * a + 1] - X64[3 * b + 1], dz = X64[3 * a + 2] - X64[3 * b + 2];
+    double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 <= k.cut2) sg += gb_pair64(qa * q64[b], r2, Ra * RC[2 * b], k);
   }
   long long o = (long long)f * nR + a;
-  rows[2 * o] = sv;
-  rows[2 * o + 1] = se;
+  rows[3 * o] = sv;
+  rows[3 * o + 1] = se;
+  rows[3 * o + 2] = sg;
 }
 
 __global__ void k_rl_cols(int nC, int nR, const double* __restrict__ xyz64, const double* __restrict__ q64,
@@ -691,17 +764,21 @@ __global__ void k_reduce(int nC, int nR, int nb1, int ntiles, int nbp, const dou
     double q = q64[s];
     v[14] += fabs(f0 * q * q / R[0] - f0 * q * q / R[1]);  // decomposition.rs:320-337
   }
-  for (int a = threadIdx.x; a < nR; a += blockDim.x) v[15] += rows[((long long)f * nR + a) * 2] + rows[((long long)f * nR + a) * 2 + 1];
+  for (int a = threadIdx.x; a < nR; a += blockDim.x) {
+    v[15] += rows[((long long)f * nR + a) * 3] + rows[((long long)f * nR + a) * 3 + 1];
+    v[21] += rows[((long long)f * nR + a) * 3 + 2];
+  }
   for (int b = threadIdx.x; b < nbp; b += blockDim.x)
     for (int q = 0; q < 5; q++) v[16 + q] += bpart[((long long)f * nbp + b) * 5 + q];
-  for (int q = 0; q < 21; q++) {
+  for (int q = 0; q < 22; q++) {
     double s = block_sum(v[q], sh);
     if (threadIdx.x == 0) tot[q] = s;
   }
   __syncthreads();
   double selfC = tot[0], selfR = tot[1], selfL = tot[2], dself = tot[3];
   // pair sums count each unordered pair once; the reference adds 2 x pair (gb_energy.rs:348)
-  double gbC = 2.0 * tot[4], gbR = 2.0 * tot[5], gbL = 2.0 * tot[6], dgb = 2.0 * tot[7], mmR = tot[8], mmL = tot[9];
+  double gbC = 2.0 * tot[4], gbR = 2.0 * tot[5], gbL = 2.0 * tot[6], dgb = 2.0 * (tot[7] + tot[21]), mmR = tot[8],
+         mmL = tot[9];
   double SC = tot[10], SR = tot[11], SL = tot[12], dS = tot[13], tw = tot[14], eRL = tot[15];
   double bR = tot[16], bL = tot[17], bX = tot[18], cR = tot[19], cL = tot[20];
   double d_polar = dself + dgb;
@@ -728,7 +805,7 @@ __global__ void k_reduce(int nC, int nR, int nb1, int ntiles, int nbp, const dou
     double w = 0.0;
     for (int k = res_ptr[r]; k < res_ptr[r + 1]; k++) {
       int s = res_slots[k];
-      const double* rc = s < nR ? rows + ((long long)f * nR + s) * 2 : cols + ((long long)f * nL + (s - nR)) * 2;
+      const double* rc = s < nR ? rows + ((long long)f * nR + s) * 3 : cols + ((long long)f * nL + (s - nR)) * 2;
       x.vdw += 0.5 * rc[0];
       x.elec += 0.5 * rc[1];
       const double* R = R64 + ((long long)f * nC + s) * 2;
@@ -840,7 +917,7 @@ int64_t System::footprint(int64_t F) const {
     int64_t fpb = pb_frames_per_batch > 0 ? std::min(F, pb_frames_per_batch) : std::min<int64_t>(F, 16);
     pb = fpb * pb_points_estimate() * 110;
   }
-  int64_t per = n_top * 24 + nC * (24 + 16 + 16 + 8 + 8 + 4 + (int64_t)nbr_cap * 4 + 16) + nR * 16 + nL * 16 +
+  int64_t per = n_top * 24 + nC * (24 + 16 + 16 + 4 + 8 + 8 + 4 + (int64_t)nbr_cap * 4 + 16) + nR * 24 + nL * 16 +
                 (n_res_rec + n_res_lig) * 32 + 256;
   int64_t nb = (nC + kTile - 1) / kTile;
   per += nb * (nb + 1) / 2 * 48 + nb * 32;
@@ -1089,12 +1166,13 @@ void System::ensure_buffers(int64_t frames) {
   xyz32 = DevBuf(B * nC * 16, st);
   R64 = DevBuf(B * nC * 16, st);
   Rf = DevBuf(B * nC * 16, st);
+  dRf = DevBuf(B * nC * 4, st);
   nbr = DevBuf(B * nC * (int64_t)nbr_cap * 4, st);
   nbrcnt = DevBuf(B * nC * 4, st);
   sasa = DevBuf(B * nC * 16, st);
   k1part = DevBuf(B * nb1 * 4 * 8, st);
   k2part = DevBuf(B * (int64_t)fp->ntiles * 6 * 8, st);
-  rows = DevBuf(B * std::max<int64_t>(nR, 1) * 16, st);
+  rows = DevBuf(B * std::max<int64_t>(nR, 1) * 24, st);
   cols = DevBuf(B * std::max<int64_t>(nL, 1) * 16, st);
   bpart = DevBuf(B * nbp * 5 * 8, st);
   res_buf = DevBuf(B * sizeof(rstg_frame_energy), st);
@@ -1142,12 +1220,13 @@ void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_
                                                    P.P32.as<float4>(), P.rho64.as<double>(), P.sj64.as<double>(),
                                                    P.rad64.as<double>(), P.q64.as<double>(), P.gb,
                                                    (float)P.probe, nbr_cap, nbr.as<int>(), nbrcnt.as<int>(),
-                                                   R64.as<double>(), Rf.as<float4>(), k1part.as<double>(),
+                                                   R64.as<double>(), Rf.as<float4>(), dRf.as<float>(), k1part.as<double>(),
                                                    diag.as<int>());
   mark("psi", Fd * nCd * (nCd - 1) * 32.0, 0.0);
   size_t ljsm = (size_t)P.nt * P.nt * sizeof(float2);
   k_pairs<<<dim3((unsigned)P.ntiles, Fu), kTile, ljsm, st>>>(
-      (int)nC, (int)nR, P.tiles.as<int4>(), xyz32.as<float4>(), xyz64.as<double>(), Rf.as<float4>(), P.type.as<int>(),
+      (int)nC, (int)nR, P.tiles.as<int4>(), xyz32.as<float4>(), xyz64.as<double>(), Rf.as<float4>(), dRf.as<float>(),
+      P.type.as<int>(),
       P.nt, P.lj32.as<float2>(), P.lj64.as<double2>(), P.masks.as<unsigned>(), P.gb, split.complex.scee,
       split.complex.scnb, k2part.as<double>(), diag.as<int>());
   mark("pairs", Fd * (nCd * (nCd - 1) / 2 * gbf + same_pairs * (gbf + 22.0)), 0.0);
@@ -1161,7 +1240,8 @@ void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_
   if (nR > 0 && nL > 0) {
     k_rl_rows<<<dim3((unsigned)((nR + 127) / 128), Fu), 128, 0, st>>>(
         (int)nC, (int)nR, xyz64.as<double>(), P.q64.as<double>(), P.type.as<int>(), P.nt, P.lj64.as<double2>(),
-        P.tile_rec.as<int>(), P.nb, P.masks.as<unsigned>(), split.complex.scee, split.complex.scnb, rows.as<double>());
+        P.tile_rec.as<int>(), P.nb, P.masks.as<unsigned>(), split.complex.scee, split.complex.scnb, R64.as<double>(),
+        P.gb, rows.as<double>());
     mark("rl_rows", Fd * nRd * nLd * 22.0, 0.0);
     k_rl_cols<<<dim3((unsigned)((nL + 7) / 8), Fu), 256, 0, st>>>(
         (int)nC, (int)nR, xyz64.as<double>(), P.q64.as<double>(), P.type.as<int>(), P.nt, P.lj64.as<double2>(),
@@ -1196,7 +1276,7 @@ void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_
 void System::release_buffers() {
   if (graph) cudaGraphExecDestroy(graph);
   graph = nullptr;
-  for (DevBuf* b : {&in_frames, &xyz64, &xyz32, &R64, &Rf, &nbr, &nbrcnt, &sasa, &k1part, &k2part, &rows, &cols, &bpart,
+  for (DevBuf* b : {&in_frames, &xyz64, &xyz32, &R64, &Rf, &dRf, &nbr, &nbrcnt, &sasa, &k1part, &k2part, &rows, &cols, &bpart,
                     &res_buf, &dec_buf, &diag})
     *b = DevBuf();
   buf_frames = 0;

@@ -36,7 +36,7 @@ struct System {
   int nbr_cap = 320;
 
   // per-batch buffers (fused)
-  DevBuf in_frames, xyz64, xyz32, R64, Rf, nbr, nbrcnt, sasa, k1part, k2part, rows, cols, bpart, res_buf, dec_buf,
+  DevBuf in_frames, xyz64, xyz32, R64, Rf, dRf, nbr, nbrcnt, sasa, k1part, k2part, rows, cols, bpart, res_buf, dec_buf,
       diag;
   int64_t buf_frames = 0;
   cudaGraphExec_t graph = nullptr;
