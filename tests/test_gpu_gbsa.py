@@ -366,3 +366,31 @@ def test_sharded_frames_equal_single_process(rst, sysdata):
     st = SH.statistics(rows)
     d = rows[:, 12]
     assert abs(st["mean_delta_total"] - d.mean()) < 1e-9 and abs(st["std_delta_total"] - d.std(ddof=1)) < 1e-9
+
+
+@pytest.fixture(scope="module")
+def w2(tmp_path_factory):
+    from rust_simulation_tools import synthetic as S
+
+    d = tmp_path_factory.mktemp("w2")
+    s, fr = S.workload(2, n_frames=3)
+    S.write_prmtop(s, str(d / "w2.prmtop"))
+    return s, fr, str(d / "w2.prmtop")
+
+
+def test_fused_binding_terms_at_workload_size(rst, oracle, w2):
+    # 5,050 atoms (12.7 M pairs per frame): the binding GB difference is
+    # formed from per-pair differences, so it stays far inside 1e-3 kcal/mol
+    # of the FP64 form (guard 1e-4); delta_mm against the accurate restatement
+    s, fr, prm = w2
+    top, otop = rst.read_prmtop(prm), oracle.Topology.load(prm)
+    kw = dict(gb_params=rst.GbParams(model=2, solvent_dielectric=78.5), sa_params=rst.SaParams(n_sphere_points=960))
+    fused = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, **kw).run(fr)
+    plain = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, mode="plain", **kw).run(fr)
+    assert np.abs(fused[:, 10] - plain[:, 10]).max() < 1e-4
+    assert np.abs(fused[:, 11] - plain[:, 11]).max() < 1e-9
+    acc = oracle.binding_frame(otop, dcd_coords(fr[0]), s.receptor_residues, s.ligand_residues,
+                               gb=oracle.gb_params("obc2", solvent_dielectric=78.5),
+                               sa=oracle.sa_params(n_points=960), accurate=True)
+    assert abs(fused[0, 9] - acc["delta_mm"]) < 1e-3
+    assert abs(fused[0, 10] - acc["delta_polar"]) < 1e-3
