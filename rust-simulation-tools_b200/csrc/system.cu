@@ -181,6 +181,7 @@ __global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __r
     __syncthreads();
     int m = min(kTile, nC - j0);
     float po = 0.f, pc = 0.f;
+    unsigned nearm[kTile / 32] = {0, 0, 0, 0};  // tile columns that take the FP64 near path
     if (valid) {
       for (int jj = 0; jj < m; jj++) {
         int j = j0 + jj;
@@ -203,6 +204,18 @@ __global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __r
           else
             pc += t;
         } else {
+          nearm[jj >> 5] |= 1u << (jj & 31);
+        }
+      }
+      // near pairs of this tile, each thread over its own set (a warp runs as
+      // many FP64 evaluations as its busiest lane, not one per column any
+      // lane needs)
+      for (int w = 0; w < kTile / 32; w++) {
+        unsigned mk = nearm[w];
+        while (mk) {
+          int b = __ffs(mk) - 1;
+          mk &= mk - 1;
+          int j = j0 + 32 * w + b;
           near64++;
           double ddx = X64[3 * i] - X64[3 * j], ddy = X64[3 * i + 1] - X64[3 * j + 1],
                  ddz = X64[3 * i + 2] - X64[3 * j + 2];
@@ -211,7 +224,7 @@ __global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __r
           bool used;
           double t = hct64(rr2, rho_i64, sj64[j], used);
           if (used) {
-            if (own)
+            if ((j < nR) == in_r)
               psi_own += t;
             else
               psi_oth += t;
