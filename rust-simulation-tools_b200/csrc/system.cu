@@ -481,6 +481,8 @@ __global__ void k_sasa(int nC, int nR, int cap, const int* __restrict__ nbr, con
   int* val = sval + w * cap2;
   long long o = (long long)f * nC + i;
   int cnt = min(nbrcnt[o], cap);
+  int c2 = 32;  // sort length: this atom's neighbours rounded up to a power of two
+  while (c2 < cnt) c2 <<= 1;
   const int* L = nbr + o * cap;
   const float4* X = xyz32 + (long long)f * nC;
   const double* X64 = xyz64 + (long long)f * nC * 3;
@@ -491,7 +493,7 @@ __global__ void k_sasa(int nC, int nR, int cap, const int* __restrict__ nbr, con
   // all of them) exit after a test or two.  Order does not change which
   // points are accessible.
   int n_own = 0;
-  for (int k = lane; k < cap2; k += 32) {
+  for (int k = lane; k < c2; k += 32) {
     if (k < cnt) {
       int j = L[k];
       float4 xj = X[j];
@@ -510,9 +512,9 @@ __global__ void k_sasa(int nC, int nR, int cap, const int* __restrict__ nbr, con
     n_own += __popc(__ballot_sync(0xffffffffu, own));
   }
   __syncwarp();
-  for (int size = 2; size <= cap2; size <<= 1)  // bitonic sort of (key, val)
+  for (int size = 2; size <= c2; size <<= 1)  // bitonic sort of (key, val)
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int t = lane; t < cap2 / 2; t += 32) {
+      for (int t = lane; t < c2 / 2; t += 32) {
         int a = 2 * t - (t & (stride - 1)), b = a + stride;
         bool up = (a & size) == 0;
         float ka = key[a], kb = key[b];
