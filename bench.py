@@ -338,10 +338,22 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--pb-frames", type=int, default=32, help="MM-PBSA leg frames (0: skip)")
     ap.add_argument("--no-large", action="store_true", help="skip the 25,080-atom mixed GB/PB serving leg")
+    ap.add_argument("--pb-only", action="store_true", help="run only the MM-PBSA leg (--pb-frames frames) and print it")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e/plain/cpu/serving legs")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.pb_only:
+        import torch
+
+        import rust_simulation_tools as rst
+        from rust_simulation_tools import _native as N
+
+        torch.cuda.set_device(0)
+        ctx = N.make_ctx(0, torch.cuda.current_stream().cuda_stream)
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        print(json.dumps(pbsa_leg(rst, ctx, args.pb_frames, 1, peak)), flush=True)
         return
 
     import torch
