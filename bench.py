@@ -208,9 +208,10 @@ def _fifo_latencies(arrivals, service):
 
 def serving_stream(rst, ctx, n_req, seed=4):
     """Bounded mixed stream: receptors log-uniform 1k-20k atoms, ligands
-    20-80 atoms, 1-200 frames per request, Poisson arrivals; beside it the
-    same requests one at a time (fused engine, and plain FP64 form from its
-    per-frame time on each system) on the same arrival times."""
+    20-80 atoms, 1-200 frames per request, Poisson arrivals at 70 % of the
+    one-at-a-time capacity; beside it the same requests one at a time (fused
+    engine, and plain FP64 form from its per-frame time on each system) on the
+    same arrival times."""
     from rust_simulation_tools import synthetic as S
 
     rng = np.random.default_rng(seed)
@@ -233,9 +234,17 @@ def serving_stream(rst, ctx, n_req, seed=4):
         reqs.append((k, S.make_frames(systems[k][0], int(rng.integers(1, 201)), seed=int(rng.integers(1 << 30)))))
     for s, bs, bp, _ in systems:  # first-use preparation outside the stream
         bs.run(S.make_frames(s, 1, seed=1))
+    # one request at a time through the fused engine (measured service times)
+    svc = []
+    for k, fr in reqs:
+        t = time.perf_counter()
+        systems[k][1].run(fr)
+        svc.append(time.perf_counter() - t)
+    # Poisson arrivals at 70 % of the one-at-a-time capacity, so the queue is
+    # stable and latency measures scheduling rather than an overload backlog
+    mean_gap = sum(svc) / n_req / 0.7
+    arrivals = np.cumsum(rng.exponential(mean_gap, size=n_req))
     srv = rst.Server(max_inflight=4, ctx=ctx)
-    gaps = rng.exponential(0.01, size=n_req)
-    arrivals = np.cumsum(gaps)
     t0 = time.perf_counter()
     ids = []
     for (k, fr), a in zip(reqs, arrivals):
@@ -249,12 +258,6 @@ def serving_stream(rst, ctx, n_req, seed=4):
     st = srv.stats()
     srv.close()
     frames = sum(fr.shape[0] for _, fr in reqs)
-    # one request at a time through the fused engine (measured service times)
-    svc = []
-    for k, fr in reqs:
-        t = time.perf_counter()
-        systems[k][1].run(fr)
-        svc.append(time.perf_counter() - t)
     lat = _fifo_latencies(arrivals, svc)
     # plain FP64 form: per-frame time of each system on 2 frames
     per_frame = []
@@ -267,16 +270,18 @@ def serving_stream(rst, ctx, n_req, seed=4):
     psvc = [per_frame[k] * fr.shape[0] for k, fr in reqs]
     plat = _fifo_latencies(arrivals, psvc)
     return {"requests": n_req, "frames": frames, "receptor_atoms": [int(x[3]) for x in systems],
-            "continuous_batching": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "frames_per_s": frames / wall},
+            "continuous_batching": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                                    "delivered_frames_per_s": frames / wall,
+                                    "note": "delivered rate follows the offered load (70 % of one-at-a-time capacity)"},
             "one_at_a_time_fused": {"p50_ms": 1e3 * float(np.percentile(lat, 50)),
                                     "p99_ms": 1e3 * float(np.percentile(lat, 99)),
-                                    "frames_per_s": frames / sum(svc)},
+                                    "capacity_frames_per_s": frames / sum(svc)},
             "one_at_a_time_plain_fp64": {"p50_ms": 1e3 * float(np.percentile(plat, 50)),
                                          "p99_ms": 1e3 * float(np.percentile(plat, 99)),
-                                         "frames_per_s": frames / sum(psvc),
+                                         "capacity_frames_per_s": frames / sum(psvc),
                                          "how": "per-frame time of each system measured on 2 frames; FIFO queue "
                                                 "on the same arrival times"},
-            "arrival_mean_ms": 10.0}
+            "arrival_mean_ms": 1e3 * mean_gap, "load": 0.7}
 
 
 def large_mixed(rst, ctx, gb_requests=6, gb_frames=24, pb_requests=2, pb_frames=2, seed=5):

@@ -355,7 +355,9 @@ rstg_status rstg_binding_trajectory(rstg_ctx* ctx, const rstg_topology* t, const
 /* ---- serving loop -------------------------------------------------------- */
 
 typedef struct rstg_server_opts {
-  int64_t memory_budget_bytes; /* admission limit on device bytes in flight      */
+  int64_t memory_budget_bytes; /* limit on the batch buffers systems keep resident
+                                  between requests; idle systems are evicted,
+                                  least recently used first, to admit a request */
   int32_t max_inflight;        /* requests running concurrently (device streams) */
   int64_t chunk_frames;        /* frames per scheduling quantum                 */
 } rstg_server_opts;
@@ -363,8 +365,9 @@ void rstg_server_opts_default(rstg_server_opts* o);
 
 rstg_status rstg_server_create(rstg_ctx* ctx, const rstg_server_opts* opts, rstg_server** out);
 void rstg_server_destroy(rstg_server* s);
-/* Asynchronous: copies frames, returns a request id.  The system must outlive
- * the request. */
+/* Asynchronous: copies frames, returns a request id.  The system keeps its
+ * batch buffers between requests (reused by its next request), so a system
+ * submitted to a server must outlive the server. */
 rstg_status rstg_server_submit(rstg_server* s, rstg_system* sys, const float* frames, int64_t n_frames,
                                int64_t* request_id);
 /* RSTG_ERR_NOT_READY while running; RSTG_OK copies results (out [F]). */

@@ -5,6 +5,7 @@
 // device, and per-request latency (submit -> results ready) is recorded.
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -43,7 +44,14 @@ struct Server {
   std::vector<std::thread> slots;
   std::vector<cudaStream_t> streams;
   std::map<System*, int> busy;  // systems with a running request
-  int64_t bytes_inflight = 0, peak_bytes = 0, next_id = 1, frames_done = 0;
+  // Device bytes each system holds between requests (its batch buffers stay
+  // resident so that its next request reuses them and its captured graph);
+  // idle systems are evicted, least recently used first, when an admission
+  // needs the room.
+  std::map<System*, int64_t> resident;
+  std::map<System*, int64_t> last_use;
+  int64_t use_clock = 0;
+  int64_t resident_total = 0, peak_bytes = 0, next_id = 1, frames_done = 0;
   int running = 0;
   bool stop = false;
   std::vector<double> latencies_ms;
@@ -102,14 +110,41 @@ struct Server {
     give_streams(ctx->device, streams);
   }
 
+  int64_t growth(const Request& r) {
+    auto it = resident.find(r.sys);
+    return std::max<int64_t>(0, r.bytes - (it == resident.end() ? 0 : it->second));
+  }
+
+  // Releases idle systems' buffers (least recently used first) until `need`
+  // more bytes fit the budget; systems whose lock is taken are skipped.
+  void evict_for(int64_t need, System* keep) {
+    while (resident_total + need > opts.memory_budget_bytes) {
+      System* victim = nullptr;
+      int64_t oldest = INT64_MAX;
+      for (auto& kv : resident)
+        if (kv.first != keep && !busy.count(kv.first) && last_use[kv.first] < oldest) {
+          oldest = last_use[kv.first];
+          victim = kv.first;
+        }
+      if (!victim) return;
+      std::unique_lock<std::recursive_mutex> vl(victim->mu, std::try_to_lock);
+      if (vl.owns_lock() && victim->opts.mode == RSTG_MODE_FUSED) victim->release_buffers();
+      resident_total -= resident[victim];
+      resident.erase(victim);
+    }
+  }
+
   // Next admissible request: first in arrival order whose system is idle and
-  // whose footprint fits the budget (a request larger than the whole budget
-  // is admitted alone when nothing else runs, so it cannot starve).
+  // whose buffers fit the budget after evicting idle systems (a request
+  // larger than the whole budget is admitted alone when nothing else runs,
+  // so it cannot starve).
   std::shared_ptr<Request> pick() {
     for (auto it = queue.begin(); it != queue.end(); ++it) {
       auto& r = *it;
       if (busy.count(r->sys)) continue;
-      bool fits = bytes_inflight + r->bytes <= opts.memory_budget_bytes || running == 0;
+      int64_t need = growth(*r);
+      evict_for(need, r->sys);
+      bool fits = resident_total + need <= opts.memory_budget_bytes || running == 0;
       if (!fits) continue;
       auto q = r;
       queue.erase(it);
@@ -128,8 +163,11 @@ struct Server {
         if (!r) return;
         r->state = Request::RUNNING;
         busy[r->sys] = 1;
-        bytes_inflight += r->bytes;
-        peak_bytes = std::max(peak_bytes, bytes_inflight);
+        int64_t g = growth(*r);
+        resident[r->sys] += g;
+        resident_total += g;
+        last_use[r->sys] = ++use_clock;
+        peak_bytes = std::max(peak_bytes, resident_total);
         running++;
       }
       rstg_status st = RSTG_OK;
@@ -145,7 +183,6 @@ struct Server {
           throw;
         }
         r->sys->stream_ = prev;
-        if (r->sys->opts.mode == RSTG_MODE_FUSED) r->sys->release_buffers();
       } catch (const Error& e) {
         st = e.code;
         msg = e.what();
@@ -157,7 +194,6 @@ struct Server {
         std::lock_guard<std::mutex> lk(mu);
         r->finished = Clock::now();
         busy.erase(r->sys);
-        bytes_inflight -= r->bytes;
         running--;
         if (r->state == Request::CANCELLED) {
           r->out.clear();

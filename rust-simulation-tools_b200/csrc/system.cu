@@ -1172,6 +1172,10 @@ void System::prepare_fused(const double* x0) {
 
 void System::ensure_buffers(int64_t frames) {
   if (frames <= buf_frames) return;
+  if (graph) {  // a captured graph holds the old buffers' addresses and capacities
+    cudaGraphExecDestroy(graph);
+    graph = nullptr;
+  }
   cudaStream_t st = stream();
   int64_t B = frames;
   int nb1 = (int)((nC + kTile - 1) / kTile);
