@@ -26,11 +26,22 @@
 // changes state; the host reads the per-grid states once per chunk.
 //
 // Layout in HBM: one FP64 pool (phi, rho and, for solvated grids, the four
-// face-dielectric / kbar^2 maps, each g.n() doubles) and one FP32 pool (per
+// face-dielectric / kbar^2 maps, each g.n() doubles), one FP32 pool (per
 // multigrid level: correction, right-hand side, residual and the four maps
-// of solvated grids).  Reference grids have a uniform dielectric and no
-// salt term, so their stencil is the constant-coefficient Laplacian and they
-// carry no maps.
+// of solvated grids) and one byte of stencil code per point and level.
+// Reference grids have a uniform dielectric and no salt term, so their
+// stencil is the constant-coefficient Laplacian and they carry no maps.
+//
+// Stencil codes: a face dielectric is eps_in on both sides of the molecular
+// surface's interior, eps_out outside, and a harmonic mean only on the edges
+// that cross the surface (pb_grid.rs:809-817); kbar^2 is 0 or one constant
+// (assign_kappa, pb_grid.rs:951-985).  Per point one byte holds, for the
+// x, y and z faces, 0 = eps_out, 1 = eps_in, 2 = read the map (bits 0-5),
+// kbar^2 != 0 (bit 6) and, at level 0, rho != 0 (bit 7).  The kernels read
+// the byte and touch a map or rho only where the code says so, with the
+// same values and the same arithmetic as reading the maps everywhere: the
+// results are bit-identical, and a solvated colour pass streams 11 bytes per
+// point instead of 26.
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
@@ -48,6 +59,7 @@ namespace rstg {
 namespace {
 
 constexpr int kMaxLev = 16;
+static_assert(kProfLevels >= kMaxLev, "profile table must cover every level");
 constexpr double kFourPiEcB = 4.0 * kPi * 332.0522;  // pb_solver.rs:155
 constexpr int kT = 256;
 
@@ -58,6 +70,8 @@ struct JobD {
   double* phi;
   const double* rho;
   const double *ex, *ey, *ez, *k2;
+  const uint8_t* cd;      // level-0 stencil codes
+  double din, dout, dkb;  // eps_in, eps_out, the non-zero kbar^2
   const double *axyz, *aq;
   int nx, ny, nz, uniform;
   int na, want_e, maxv, pad;
@@ -69,8 +83,10 @@ struct JobD {
 struct LvlD {
   float *e, *rhs, *res;  // correction, right-hand side, residual
   const float *ex, *ey, *ez, *k2;
+  const uint8_t* cd;     // stencil codes
   int nx, ny, nz, uniform;
   float ih, om, eps, pad;
+  float fin, fout, kb, pad2;
 };
 
 struct JobState {
@@ -105,9 +121,10 @@ __device__ __forceinline__ int wl_job(const WL& w, int b, int& lb) {
 struct Lv {
   float *__restrict__ e, *__restrict__ rhs, *__restrict__ res;
   const float *__restrict__ ex, *__restrict__ ey, *__restrict__ ez, *__restrict__ k2;
+  const uint8_t* __restrict__ cd;
   int nx, ny, nz, sy, sz;
   bool uni;
-  float ih, om, w6;
+  float ih, om, w6, fin, fout, kb;
 };
 __device__ __forceinline__ Lv lv_load(const LvlD* __restrict__ L, int j, int lvl) {
   const LvlD& d = L[j * kMaxLev + lvl];
@@ -119,6 +136,7 @@ __device__ __forceinline__ Lv lv_load(const LvlD* __restrict__ L, int j, int lvl
   v.ey = d.ey;
   v.ez = d.ez;
   v.k2 = d.k2;
+  v.cd = d.cd;
   v.nx = d.nx;
   v.ny = d.ny;
   v.nz = d.nz;
@@ -128,7 +146,16 @@ __device__ __forceinline__ Lv lv_load(const LvlD* __restrict__ L, int j, int lvl
   v.ih = d.ih;
   v.om = d.om;
   v.w6 = d.eps * d.ih;
+  v.fin = d.fin;
+  v.fout = d.fout;
+  v.kb = d.kb;
   return v;
+}
+
+// Face dielectric from a 2-bit stencil code: 0 eps_out, 1 eps_in, 2 the map.
+template <typename T>
+__device__ __forceinline__ T face(unsigned c, const T* __restrict__ m, int i, T ein, T eout) {
+  return c == 0u ? eout : (c == 1u ? ein : m[i]);
 }
 
 // Brick of 32 x 8 x 8 points for a 256-thread block: thread (lane, warp) owns
@@ -151,9 +178,14 @@ __device__ __forceinline__ void st32(const Lv& d, const float* __restrict__ e, i
     ns = d.w6 * ((e[i + 1] + e[i - 1]) + (e[i + sy] + e[i - sy]) + (e[i + sz] + e[i - sz]));
     dg = 6.0f * d.w6;
   } else {
-    float a = d.ex[i], b = d.ex[i - 1], c = d.ey[i], dd = d.ey[i - sy], f = d.ez[i], g = d.ez[i - sz];
+    const unsigned c0 = d.cd[i];
+    float a = face(c0 & 3u, d.ex, i, d.fin, d.fout), b = face(d.cd[i - 1] & 3u, d.ex, i - 1, d.fin, d.fout),
+          c = face((c0 >> 2) & 3u, d.ey, i, d.fin, d.fout),
+          dd = face((d.cd[i - sy] >> 2) & 3u, d.ey, i - sy, d.fin, d.fout),
+          f = face((c0 >> 4) & 3u, d.ez, i, d.fin, d.fout),
+          g = face((d.cd[i - sz] >> 4) & 3u, d.ez, i - sz, d.fin, d.fout);
     ns = ((a * e[i + 1] + b * e[i - 1]) + (c * e[i + sy] + dd * e[i - sy]) + (f * e[i + sz] + g * e[i - sz])) * d.ih;
-    dg = ((a + b) + (c + dd) + (f + g)) * d.ih + d.k2[i];
+    dg = ((a + b) + (c + dd) + (f + g)) * d.ih + ((c0 & 64u) ? d.kb : 0.0f);
   }
 }
 
@@ -170,7 +202,9 @@ __global__ void __launch_bounds__(256) k_res64(WL w, const JobD* __restrict__ J,
   float* __restrict__ rhs0 = L[j * kMaxLev].rhs;
   const double* __restrict__ p = d.phi;
   const double* __restrict__ rho = d.rho;
-  const double *__restrict__ ex = d.ex, *__restrict__ ey = d.ey, *__restrict__ ez = d.ez, *__restrict__ kk = d.k2;
+  const double *__restrict__ ex = d.ex, *__restrict__ ey = d.ey, *__restrict__ ez = d.ez;
+  const uint8_t* __restrict__ cd = d.cd;
+  const double din = d.din, dout = d.dout, dkb = d.dkb;
   const bool uni = d.uniform != 0;
   const double ih = d.ih, wt = d.eps * d.ih;
   const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny;
@@ -183,17 +217,21 @@ __global__ void __launch_bounds__(256) k_res64(WL w, const JobD* __restrict__ J,
       int z = z0 + k;
       if (z < 1 || z > nz - 2) continue;
       int i = x + sy * y + sz * z;
+      const unsigned c0 = cd[i];
       double ns, dg;
       if (uni) {
         ns = wt * ((p[i + 1] + p[i - 1]) + (p[i + sy] + p[i - sy]) + (p[i + sz] + p[i - sz]));
         dg = 6.0 * wt;
       } else {
-        double a = ex[i], b = ex[i - 1], c = ey[i], dd = ey[i - sy], f = ez[i], g = ez[i - sz];
+        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[i - 1] & 3u, ex, i - 1, din, dout),
+               c = face((c0 >> 2) & 3u, ey, i, din, dout), dd = face((cd[i - sy] >> 2) & 3u, ey, i - sy, din, dout),
+               f = face((c0 >> 4) & 3u, ez, i, din, dout), g = face((cd[i - sz] >> 4) & 3u, ez, i - sz, din, dout);
         ns = (a * p[i + 1] + b * p[i - 1]) * ih + (c * p[i + sy] + dd * p[i - sy]) * ih +
              (f * p[i + sz] + g * p[i - sz]) * ih;
-        dg = (a + b) * ih + (c + dd) * ih + (f + g) * ih + kk[i];
+        dg = (a + b) * ih + (c + dd) * ih + (f + g) * ih + ((c0 & 64u) ? dkb : 0.0);
       }
-      double r = kFourPiEcB * rho[i] + ns - dg * p[i];
+      double q = (c0 & 128u) ? rho[i] : 0.0;
+      double r = kFourPiEcB * q + ns - dg * p[i];
       rhs0[i] = (float)r;
       acc += r * r;
     }
@@ -273,29 +311,42 @@ __global__ void __launch_bounds__(256) k_update64(WL w, const JobD* __restrict__
   }
 }
 
-// One colour of a red-black SOR sweep on one level (pb_solver.rs:250-317),
-// one point of the colour per thread.  Each colour pass streams the level's
-// arrays once; at the batch sizes used here this runs at the HBM copy rate,
-// which a single-pass (both colours) brick with halo staging did not reach.
+// One colour of a red-black SOR sweep on one level (pb_solver.rs:250-317).
+// Thread k of a block row owns the colour's point (2t + parity, y) of the
+// (x, y) plane in kRbZ consecutive z planes.  Points of one colour do not
+// read each other, so all loads of the thread's points are issued before its
+// first store and are in flight together, and the job lookup and index
+// decode are paid once per kRbZ points (the pass is issue- and
+// latency-bound, not DRAM-bound, at one point per thread).
+constexpr int kRbZ = 4;
 __global__ void __launch_bounds__(256) k_rb32(WL w, const LvlD* __restrict__ L, int lvl,
                                               const JobState* __restrict__ S, int colour) {
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != kMg) return;
   const Lv d = lv_load(L, j, lvl);
-  int hw = (d.nx - 1) >> 1, nyi = d.ny - 2;
-  int cnt = hw * nyi * (d.nz - 2);
-  int k = lb * blockDim.x + threadIdx.x;
-  if (k >= cnt) return;
-  int t = k % hw, row = k / hw;
-  int iy = 1 + row % nyi, iz = 1 + row / nyi;
-  int ix = 1 + ((1 + iy + iz + colour) & 1) + 2 * t;
-  if (ix >= d.nx - 1) return;
-  int i = ix + d.sy * iy + d.sz * iz;
-  float ns, dg;
-  st32(d, d.e, i, ns, dg);
-  float old = d.e[i];
-  float gs = __fdividef(ns + d.rhs[i], dg);
-  d.e[i] = old + d.om * (gs - old);
+  const int hw = (d.nx - 1) >> 1, plane = hw * (d.ny - 2);
+  const int nbp = (plane + kT - 1) / kT, bz = lb / nbp;
+  const int k = (lb - bz * nbp) * kT + threadIdx.x;
+  if (k >= plane) return;
+  const int t = k % hw, iy = 1 + k / hw, z0 = 1 + bz * kRbZ;
+  float ns[kRbZ], dg[kRbZ], ev[kRbZ], rv[kRbZ];
+  int idx[kRbZ];
+#pragma unroll
+  for (int r = 0; r < kRbZ; r++) {
+    const int z = z0 + r, ix = 1 + ((1 + iy + z + colour) & 1) + 2 * t;
+    idx[r] = (z <= d.nz - 2 && ix < d.nx - 1) ? ix + d.sy * iy + d.sz * z : -1;
+    if (idx[r] >= 0) {
+      st32(d, d.e, idx[r], ns[r], dg[r]);
+      ev[r] = d.e[idx[r]];
+      rv[r] = d.rhs[idx[r]];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kRbZ; r++)
+    if (idx[r] >= 0) {
+      float gs = __fdividef(ns[r] + rv[r], dg[r]);
+      d.e[idx[r]] = ev[r] + d.om * (gs - ev[r]);
+    }
 }
 
 // One colour of the plain SOR sweep (pb_solver.rs:373-447) on the level-0
@@ -575,6 +626,48 @@ __global__ void k_maps32(WL w, const JobD* __restrict__ J, const LvlD* __restric
   ((float*)l0.k2)[i] = (float)d.k2[i];
 }
 
+// Level-0 stencil codes of every grid from its FP64 maps (exact compares),
+// with per-grid counts of map reads (edges that cross the surface) and of
+// charged points for the traffic figures; bad is set if a kbar^2 value is
+// neither 0 nor the grid's constant.
+__device__ __forceinline__ unsigned fcode(double v, double ein, double eout) {
+  return v == eout ? 0u : (v == ein ? 1u : 2u);
+}
+__global__ void k_codes(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
+                        unsigned long long* __restrict__ counts, int* __restrict__ bad) {
+  int lb, j = wl_job(w, blockIdx.x, lb);
+  const JobD& d = J[j];
+  int n = d.nx * d.ny * d.nz;
+  int i = lb * blockDim.x + threadIdx.x;
+  unsigned exc = 0, chg = 0;
+  if (i < n) {
+    unsigned c = 0;
+    if (!d.uniform) {
+      unsigned a = fcode(d.ex[i], d.din, d.dout), b = fcode(d.ey[i], d.din, d.dout), e = fcode(d.ez[i], d.din, d.dout);
+      c = a | (b << 2) | (e << 4);
+      exc = (a == 2u) + (b == 2u) + (e == 2u);
+      double k = d.k2[i];
+      if (k != 0.0) {
+        if (k == d.dkb)
+          c |= 64u;
+        else
+          *bad = 1;
+      }
+    }
+    if (d.rho[i] != 0.0) {
+      c |= 128u;
+      chg = 1;
+    }
+    ((uint8_t*)L[j * kMaxLev].cd)[i] = (uint8_t)c;
+  }
+  exc = __reduce_add_sync(0xffffffffu, exc);
+  chg = __reduce_add_sync(0xffffffffu, chg);
+  if ((threadIdx.x & 31) == 0 && (exc | chg)) {
+    atomicAdd(counts + 2 * j, (unsigned long long)exc);
+    atomicAdd(counts + 2 * j + 1, (unsigned long long)chg);
+  }
+}
+
 __global__ void k_inject32(WL w, const LvlD* __restrict__ L, int lvl) {
   int lb, j = wl_job(w, blockIdx.x, lb);
   const LvlD& f = L[j * kMaxLev + lvl];
@@ -588,6 +681,7 @@ __global__ void k_inject32(WL w, const LvlD* __restrict__ L, int lvl) {
   ((float*)c.ey)[i] = f.ey[fi];
   ((float*)c.ez)[i] = f.ez[fi];
   ((float*)c.k2)[i] = f.k2[fi];
+  ((uint8_t*)c.cd)[i] = f.cd[fi] & 127u;  // maps are injected, so are their codes; no rho below level 0
 }
 
 // 0.5 sum_a q_a phi(x_a), trilinear phi (pb_solver.rs:1174-1186); one block per grid.
@@ -708,10 +802,10 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   struct Lay {
     int nlev = 0;  // coarse multigrid levels; -1: plain SOR (minimum dimension <= 8)
     PbGeom lv[kMaxLev];
-    size_t o64 = 0, o32[kMaxLev] = {};
+    size_t o64 = 0, o32[kMaxLev] = {}, o8[kMaxLev] = {};
   };
   std::vector<Lay> lay(nj);
-  size_t n64 = 0, n32 = 0;
+  size_t n64 = 0, n32 = 0, n8 = 0;
   for (int j = 0; j < nj; j++) {
     PbJob& J = jobs[j];
     Lay& Y = lay[j];
@@ -742,11 +836,18 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       size_t m = Y.lv[l].n();
       n32 += (J.uniform ? 3 : 7) * m;
       n32 = (n32 + 63) & ~(size_t)63;
+      if (l == 0 || !J.uniform) {  // codes: rho bits of every level-0 grid, stencils of solvated grids
+        Y.o8[l] = n8;
+        n8 = (n8 + m + 255) & ~(size_t)255;
+      }
     }
   }
   size_t b64 = std::max<size_t>(n64, 1) * 8, b32 = std::max<size_t>(n32, 1) * 4;
   if (pool64_.bytes < b64) pool64_ = DevBuf(b64, st);
   if (pool32_.bytes < b32) pool32_ = DevBuf(b32, st);
+  size_t b8 = std::max<size_t>(n8, 1);
+  if (pool8_.bytes < b8) pool8_ = DevBuf(b8, st);
+  uint8_t* P8 = (uint8_t*)pool8_.p;
   double* P64 = pool64_.as<double>();
   float* P32 = pool32_.as<float>();
   RSTG_CUDA(cudaMemsetAsync(P32, 0, b32, st));
@@ -823,6 +924,10 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       d.ez = base + 4 * n;
       d.k2 = base + 5 * n;
     }
+    d.cd = P8 + Y.o8[0];
+    d.din = J.ein;
+    d.dout = J.eout;
+    d.dkb = J.ionic ? p.solvent_dielectric * J.kap * J.kap : 0.0;  // assign_kappa, pb_grid.rs:964
     d.nx = J.g.nx;
     d.ny = J.g.ny;
     d.nz = J.g.nz;
@@ -863,7 +968,13 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
         L.ey = b + 4 * m;
         L.ez = b + 5 * m;
         L.k2 = b + 6 * m;
+        L.cd = P8 + Y.o8[l];
+      } else if (l == 0) {
+        L.cd = P8 + Y.o8[0];
       }
+      L.fin = (float)J.ein;
+      L.fout = (float)J.eout;
+      L.kb = (float)d.dkb;
       L.nx = g.nx;
       L.ny = g.ny;
       L.nz = g.nz;
@@ -884,18 +995,20 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   RSTG_CUDA(cudaMemcpyAsync(dS, hs.data(), sizeof(JobState) * nj, cudaMemcpyHostToDevice, st));
   size_t pbytes = (size_t)nparts * nj * 8 * 3;  // residual partials, then two colours of SOR partials
   if (part_.bytes < pbytes) part_ = DevBuf(pbytes, st);
-  if (small_.bytes < (size_t)nj * 16) small_ = DevBuf((size_t)nj * 16, st);
+  if (small_.bytes < (size_t)nj * 32 + 16) small_ = DevBuf((size_t)nj * 32 + 16, st);
   double* part = part_.as<double>();
   double* spart = part + (size_t)nparts * nj;
 
-  // FP32 maps of the solvated grids
+  // FP32 maps and stencil codes (level-0 codes of every grid: the rho bit)
+  std::vector<unsigned long long> counts(2 * (size_t)nj);
   {
     Lists setup;
-    int s0 = setup.add_slot();
+    int s0 = setup.add_slot(), sc = setup.add_slot();
     std::vector<int> si(kMaxLev);
     for (int l = 0; l + 1 < kMaxLev; l++) si[l] = setup.add_slot();
     int maxl = 0;
     for (int j = 0; j < nj; j++) {
+      setup.add(sc, j, cdiv((long long)jobs[j].g.n(), kT));
       if (jobs[j].uniform) continue;
       setup.add(s0, j, cdiv((long long)jobs[j].g.n(), kT));
       for (int l = 0; l < lay[j].nlev; l++) setup.add(si[l], j, cdiv((long long)lay[j].lv[l + 1].n(), kT));
@@ -903,6 +1016,11 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     }
     std::vector<WL> wl;
     setup.upload(lists_, st, wl);
+    unsigned long long* dcnt = (unsigned long long*)small_.p;
+    int* dbad = (int*)(dcnt + 2 * (size_t)nj);
+    RSTG_CUDA(cudaMemsetAsync(dcnt, 0, 16 * (size_t)nj + 16, st));
+    k_codes<<<setup.slots[sc].total, kT, 0, st>>>(wl[sc], dJ, dL, dcnt, dbad);
+    launched(c_);
     if (setup.slots[s0].total > 0) {
       k_maps32<<<setup.slots[s0].total, kT, 0, st>>>(wl[s0], dJ, dL);
       launched(c_);
@@ -912,7 +1030,11 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
         k_inject32<<<setup.slots[si[l]].total, kT, 0, st>>>(wl[si[l]], dL, l);
         launched(c_);
       }
+    int bad = 0;
+    RSTG_CUDA(cudaMemcpyAsync(counts.data(), dcnt, 16 * (size_t)nj, cudaMemcpyDeviceToHost, st));
+    RSTG_CUDA(cudaMemcpyAsync(&bad, dbad, 4, cudaMemcpyDeviceToHost, st));
     RSTG_CUDA(cudaStreamSynchronize(st));
+    if (bad) throw Error(RSTG_ERR_INVALID, "PB kbar^2 map holds a value other than 0 and eps_s kappa^2");
   }
   auto t1 = now();
   stats.ms_setup += ms(t0, t1);
@@ -950,12 +1072,17 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   std::vector<LvSlots> ls(kMaxLev);
   int s_upd = 0, s_res = 0, s_norm = 0, s_sres = 0, s_sor = 0, s_supd = 0, s_snorm = 0, maxlev = 0;
   bool any_mg = false, any_sor = false;
-  // profile mode: events around the level-0 kernels, with their algorithmic
-  // bytes (compulsory DRAM traffic per launch) from the current lists
+  // profile mode: events around every launch; the level-0 kernels also
+  // carry their algorithmic bytes (compulsory DRAM traffic per launch) from
+  // the current lists.  kind: roofline slot (-1 none); det: kernel family.
   double kbytes[kProfKernels] = {};
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  struct Mark {
+    int kind, det, lvl;
+    cudaEvent_t a, b;
+  };
+  std::vector<Mark> marks;
   size_t next_ev = 0;
-  auto mark = [&](int kind, auto&& launch) {
+  auto mark = [&](int kind, int det, int lvl, auto&& launch) {
     if (!profile) {
       launch();
       return;
@@ -970,60 +1097,56 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     RSTG_CUDA(cudaEventRecord(a, st));
     launch();
     RSTG_CUDA(cudaEventRecord(b, st));
-    marks.push_back({kind, {a, b}});
+    marks.push_back({kind, det, lvl, a, b});
   };
+  enum { dSweep, dRes32, dRestrict, dProlong, dCoarse, dRes64, dUpdate, dNorm, dSor };
   auto enqueue_chunk = [&]() {
     int n = 0;
     auto go = [&](int slot) { return lists.slots[slot].total; };
+    auto sweeps = [&](int l) {
+      for (int s = 0; s < 3; s++)
+        for (int colour = 0; colour < 2; colour++) {
+          mark(l == 0 ? 0 : -1, dSweep, l,
+               [&] { k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour); });
+          n++;
+        }
+    };
     for (int k = 0; k < K; k++) {
       if (any_mg) {
         for (int l = 0; l <= maxlev; l++) {
           if (go(ls[l].rb)) {
-            for (int s = 0; s < 3; s++)
-              for (int colour = 0; colour < 2; colour++) {
-                if (l == 0)
-                  mark(0, [&] { k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour); });
-                else
-                  k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour);
-                n++;
-              }
-            if (l == 0)
-              mark(1, [&] { k_res32<<<go(ls[l].res), kT, 0, st>>>(wl[ls[l].res], dL, l, dS); });
-            else
-              k_res32<<<go(ls[l].res), kT, 0, st>>>(wl[ls[l].res], dL, l, dS);
-            k_restrict32<<<go(ls[l].restr), kT, 0, st>>>(wl[ls[l].restr], dL, l, dS);
+            sweeps(l);
+            mark(l == 0 ? 1 : -1, dRes32, l, [&] { k_res32<<<go(ls[l].res), kT, 0, st>>>(wl[ls[l].res], dL, l, dS); });
+            mark(-1, dRestrict, l,
+                 [&] { k_restrict32<<<go(ls[l].restr), kT, 0, st>>>(wl[ls[l].restr], dL, l, dS); });
             n += 2;
           }
           if (go(ls[l].coarse)) {
-            k_coarse32<<<go(ls[l].coarse), 256, 0, st>>>(wl[ls[l].coarse], dL, l, dS, 50);
+            mark(-1, dCoarse, l,
+                 [&] { k_coarse32<<<go(ls[l].coarse), 256, 0, st>>>(wl[ls[l].coarse], dL, l, dS, 50); });
             n++;
           }
         }
         for (int l = maxlev - 1; l >= 0; l--) {
           if (!go(ls[l].prol)) continue;
-          k_prolong32<<<go(ls[l].prol), kT, 0, st>>>(wl[ls[l].prol], dL, l, dS);
+          mark(-1, dProlong, l, [&] { k_prolong32<<<go(ls[l].prol), kT, 0, st>>>(wl[ls[l].prol], dL, l, dS); });
           n++;
-          for (int s = 0; s < 3; s++)
-            for (int colour = 0; colour < 2; colour++) {
-              if (l == 0)
-                mark(0, [&] { k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour); });
-              else
-                k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour);
-              n++;
-            }
+          sweeps(l);
         }
-        mark(3, [&] { k_update64<<<go(s_upd), kT, 0, st>>>(wl[s_upd], dJ, dL, dS, kMg); });
-        mark(2, [&] { k_res64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, kMg, part, nparts); });
-        k_norm<<<go(s_norm), 256, 0, st>>>(wl[s_norm], dJ, dS, part, nparts, 1);
+        mark(3, dUpdate, 0, [&] { k_update64<<<go(s_upd), kT, 0, st>>>(wl[s_upd], dJ, dL, dS, kMg); });
+        mark(2, dRes64, 0, [&] { k_res64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, kMg, part, nparts); });
+        mark(-1, dNorm, 0, [&] { k_norm<<<go(s_norm), 256, 0, st>>>(wl[s_norm], dJ, dS, part, nparts, 1); });
         n += 3;
       }
       if (any_sor)
         for (int q = 0; q < KS; q++) {
-          k_res64<<<go(s_sres), kT, 0, st>>>(wl[s_sres], dJ, dL, dS, kSor, part, nparts);
-          k_sor32<<<go(s_sor), kT, 0, st>>>(wl[s_sor], dL, dS, 0, spart, nparts);
-          k_sor32<<<go(s_sor), kT, 0, st>>>(wl[s_sor], dL, dS, 1, spart, nparts);
-          k_update64<<<go(s_supd), kT, 0, st>>>(wl[s_supd], dJ, dL, dS, kSor);
-          k_sor_norm<<<go(s_snorm), 256, 0, st>>>(wl[s_snorm], dJ, dS, spart, nparts);
+          mark(-1, dSor, 0, [&] {
+            k_res64<<<go(s_sres), kT, 0, st>>>(wl[s_sres], dJ, dL, dS, kSor, part, nparts);
+            k_sor32<<<go(s_sor), kT, 0, st>>>(wl[s_sor], dL, dS, 0, spart, nparts);
+            k_sor32<<<go(s_sor), kT, 0, st>>>(wl[s_sor], dL, dS, 1, spart, nparts);
+            k_update64<<<go(s_supd), kT, 0, st>>>(wl[s_supd], dJ, dL, dS, kSor);
+            k_sor_norm<<<go(s_snorm), 256, 0, st>>>(wl[s_snorm], dJ, dS, spart, nparts);
+          });
           n += 5;
         }
     }
@@ -1055,7 +1178,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
         maxlev = std::max(maxlev, Y.nlev);
         for (int l = 0; l < Y.nlev; l++) {
           const PbGeom& a = Y.lv[l];
-          lists.add(ls[l].rb, j, cdiv((long long)((a.nx - 1) / 2) * (a.ny - 2) * (a.nz - 2), kT));
+          lists.add(ls[l].rb, j, cdiv((long long)((a.nx - 1) / 2) * (a.ny - 2), kT) * cdiv(a.nz - 2, kRbZ));
           lists.add(ls[l].res, j, nbricks(a));
           lists.add(ls[l].restr, j, nbricks(Y.lv[l + 1]));
           lists.add(ls[l].prol, j, nbricks(a));
@@ -1075,12 +1198,12 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     for (int k = 0; k < kProfKernels; k++) kbytes[k] = 0.0;
     for (int j = 0; j < nj; j++)
       if (hs[j].status == kMg) {
-        double pts = (double)jobs[j].g.n();
+        double pts = (double)jobs[j].g.n(), exc = (double)counts[2 * j], chg = (double)counts[2 * j + 1];
         bool u = jobs[j].uniform;
-        kbytes[0] += pts * (u ? 10.0 : 26.0);  // e, rhs, (4 maps), half of e written
-        kbytes[1] += pts * (u ? 12.0 : 28.0);  // e, rhs, (4 maps), res written
-        kbytes[2] += pts * (u ? 20.0 : 52.0);  // phi, rho, (4 FP64 maps), rhs written
-        kbytes[3] += pts * 24.0;               // phi and e read and written
+        kbytes[0] += pts * (u ? 10.0 : 11.0) + 4.0 * exc;  // e, rhs, (codes), half of e written; map reads
+        kbytes[1] += pts * (u ? 12.0 : 13.0) + 4.0 * exc;  // e, rhs, (codes), res written; map reads
+        kbytes[2] += pts * 13.0 + 8.0 * (exc + chg);        // phi, codes, rhs written; map and rho reads
+        kbytes[3] += pts * 24.0;                            // phi and e read and written
       }
     lists.upload(lists_, st, wl);
     if (use_graph && (any_mg || any_sor)) {
@@ -1140,10 +1263,14 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     RSTG_CUDA(cudaStreamSynchronize(st));
     for (auto& m : marks) {
       float t = 0.0f;
-      RSTG_CUDA(cudaEventElapsedTime(&t, m.second.first, m.second.second));
-      prof.ms[m.first] += t;
-      prof.bytes[m.first] += kbytes[m.first];
-      prof.launches[m.first] += 1;
+      RSTG_CUDA(cudaEventElapsedTime(&t, m.a, m.b));
+      if (m.kind >= 0) {
+        prof.ms[m.kind] += t;
+        prof.bytes[m.kind] += kbytes[m.kind];
+        prof.launches[m.kind] += 1;
+      }
+      prof.detail_ms[m.det][m.lvl] += t;
+      prof.detail_n[m.det][m.lvl] += 1;
     }
     marks.clear();
     next_ev = 0;
@@ -1159,6 +1286,15 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       std::fprintf(stderr, "pb grid %d: %dx%dx%d uniform %d status %d cycles %d sor %lld rms %.6e r0 %.6e\n", j,
                    jobs[j].g.nx, jobs[j].g.ny, jobs[j].g.nz, (int)jobs[j].uniform, hs[j].status, hs[j].cycles,
                    hs[j].sor_it, hs[j].rms, hs[j].r0);
+  if (profile && std::getenv("RSTG_PB_DEBUG")) {
+    static const char* names[kProfDetail] = {"sweep", "res32", "restrict", "prolong", "coarse",
+                                             "res64", "update", "norm",     "sor"};
+    for (int d = 0; d < kProfDetail; d++)
+      for (int l = 0; l < kProfLevels; l++)
+        if (prof.detail_n[d][l])
+          std::fprintf(stderr, "pb profile %-8s level %d: %8.2f ms over %lld launches\n", names[d], l,
+                       prof.detail_ms[d][l], (long long)prof.detail_n[d][l]);
+  }
   auto t2 = now();
   stats.ms_cycles += ms(t1, t2);
   for (int j = 0; j < nj; j++) {

@@ -38,9 +38,14 @@ struct PbBatchStats {
 // 0 colour sweep, 1 FP32 residual, 2 FP64 residual, 3 update; bytes are the
 // algorithmic (compulsory) DRAM bytes of the timed launches.
 constexpr int kProfKernels = 4;
+// Per kernel family and multigrid level: sweep, FP32 residual, restriction,
+// prolongation, coarsest level, FP64 residual, update, norm, SOR fallback.
+constexpr int kProfDetail = 9, kProfLevels = 16;
 struct PbProfile {
   double ms[kProfKernels] = {}, bytes[kProfKernels] = {};
   int64_t launches[kProfKernels] = {};
+  double detail_ms[kProfDetail][kProfLevels] = {};
+  int64_t detail_n[kProfDetail][kProfLevels] = {};
 };
 
 class PbBatchEngine {
@@ -60,7 +65,7 @@ class PbBatchEngine {
  private:
   Ctx* c_;
   cudaStream_t st_;
-  DevBuf pool64_, pool32_, desc_, part_, small_, lists_;
+  DevBuf pool64_, pool32_, pool8_, desc_, part_, small_, lists_;
   cudaGraphExec_t graph_ = nullptr;
   std::vector<cudaEvent_t> prof_events_;
 };
