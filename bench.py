@@ -131,7 +131,9 @@ PB = dict(grid_spacing=0.5, grid_buffer=12.0, fillratio=0.0)  # linearised PB, D
 
 
 def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs):
-    """MM-PBSA frames/s, batched mixed precision vs plain FP64, same frames."""
+    """MM-PBSA frames/s, batched mixed precision vs plain FP64 on the same frames
+    (per-frame solve cost varies: some frames stop at the cycle cap, some
+    diverge and finish with SOR)."""
     import torch
     from rust_simulation_tools import synthetic as S
 
@@ -358,7 +360,7 @@ def main():
         torch.cuda.set_device(0)
         ctx = N.make_ctx(0, torch.cuda.current_stream().cuda_stream)
         peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
-        print(json.dumps(pbsa_leg(rst, ctx, args.pb_frames, 1, peak)), flush=True)
+        print(json.dumps(pbsa_leg(rst, ctx, args.pb_frames, args.pb_frames, peak)), flush=True)
         return
 
     import torch
@@ -487,7 +489,7 @@ def main():
             extras["serving"] = serving_stream(rst, ctx, args.serve_requests)
         if rank == 0 and world == 1 and args.pb_frames > 0:
             peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
-            extras["pbsa"] = pbsa_leg(rst, ctx, args.pb_frames, 3, peak)
+            extras["pbsa"] = pbsa_leg(rst, ctx, args.pb_frames, args.pb_frames, peak)  # plain on the same frames
         if rank == 0 and world == 1 and not args.no_large:
             extras["large_mixed"] = large_mixed(rst, ctx)
 

@@ -74,19 +74,20 @@ struct JobD {
   double din, dout, dkb;  // eps_in, eps_out, the non-zero kbar^2
   const double *axyz, *aq;
   int nx, ny, nz, uniform;
-  int na, want_e, maxv, pad;
+  int na, want_e, maxv, px;  // px: row pitch of the FP32 / code arrays
   double ih, eps, tol, rs2;
   double ox, oy, oz, h;
   long long maxit;
 };
 
 struct LvlD {
-  float *e, *rhs, *res;  // correction, right-hand side, residual
+  float *e, *e2, *rhs, *res;  // correction (two buffers: a sweep reads one, writes the other), rhs, residual
   const float *ex, *ey, *ez, *k2;
-  const uint8_t* cd;     // stencil codes
+  const uint8_t* cd;          // stencil codes
   int nx, ny, nz, uniform;
+  int px, zc, pad1, pad2;     // row pitch (nx rounded up to 4: rows start on 16-byte boundaries), sweep z chunk
   float ih, om, eps, pad;
-  float fin, fout, kb, pad2;
+  float fin, fout, kb, pad3;
 };
 
 struct JobState {
@@ -119,10 +120,10 @@ __device__ __forceinline__ int wl_job(const WL& w, int b, int& lb) {
 // reference to the descriptor in global memory would make every global store
 // force reloads of the pointers.
 struct Lv {
-  float *__restrict__ e, *__restrict__ rhs, *__restrict__ res;
+  float *__restrict__ e, *__restrict__ e2, *__restrict__ rhs, *__restrict__ res;
   const float *__restrict__ ex, *__restrict__ ey, *__restrict__ ez, *__restrict__ k2;
   const uint8_t* __restrict__ cd;
-  int nx, ny, nz, sy, sz;
+  int nx, ny, nz, sy, sz, zc;
   bool uni;
   float ih, om, w6, fin, fout, kb;
 };
@@ -130,6 +131,7 @@ __device__ __forceinline__ Lv lv_load(const LvlD* __restrict__ L, int j, int lvl
   const LvlD& d = L[j * kMaxLev + lvl];
   Lv v;
   v.e = d.e;
+  v.e2 = d.e2;
   v.rhs = d.rhs;
   v.res = d.res;
   v.ex = d.ex;
@@ -140,8 +142,9 @@ __device__ __forceinline__ Lv lv_load(const LvlD* __restrict__ L, int j, int lvl
   v.nx = d.nx;
   v.ny = d.ny;
   v.nz = d.nz;
-  v.sy = d.nx;
-  v.sz = d.nx * d.ny;
+  v.sy = d.px;
+  v.sz = d.px * d.ny;
+  v.zc = d.zc;
   v.uni = d.uniform != 0;
   v.ih = d.ih;
   v.om = d.om;
@@ -192,7 +195,7 @@ __device__ __forceinline__ void st32(const Lv& d, const float* __restrict__ e, i
 // FP64 residual r = 4 pi ec rho + ns - dg phi at the interior points; r is
 // stored rounded to FP32 as the level-0 right-hand side and its squares are
 // summed per brick (fixed order) for the RMS test.
-__global__ void __launch_bounds__(256) k_res64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
+__global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
                                                const JobState* __restrict__ S, int want, double* __restrict__ part,
                                                int nparts) {
   __shared__ double sh[32];
@@ -207,32 +210,32 @@ __global__ void __launch_bounds__(256) k_res64(WL w, const JobD* __restrict__ J,
   const double din = d.din, dout = d.dout, dkb = d.dkb;
   const bool uni = d.uniform != 0;
   const double ih = d.ih, wt = d.eps * d.ih;
-  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny;
   int x, y, z0;
   brick_col(lb, nx, ny, x, y, z0);
   double acc = 0.0;
   if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
+    int i = x + sy * y + sz * z0, ci = x + cy * y + cz * z0;  // FP64 and padded FP32 / code indices
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
+    for (int k = 0; k < 8; k++, i += sz, ci += cz) {
       int z = z0 + k;
       if (z < 1 || z > nz - 2) continue;
-      int i = x + sy * y + sz * z;
-      const unsigned c0 = cd[i];
+      const unsigned c0 = cd[ci];
       double ns, dg;
       if (uni) {
         ns = wt * ((p[i + 1] + p[i - 1]) + (p[i + sy] + p[i - sy]) + (p[i + sz] + p[i - sz]));
         dg = 6.0 * wt;
       } else {
-        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[i - 1] & 3u, ex, i - 1, din, dout),
-               c = face((c0 >> 2) & 3u, ey, i, din, dout), dd = face((cd[i - sy] >> 2) & 3u, ey, i - sy, din, dout),
-               f = face((c0 >> 4) & 3u, ez, i, din, dout), g = face((cd[i - sz] >> 4) & 3u, ez, i - sz, din, dout);
+        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci - 1] & 3u, ex, i - 1, din, dout),
+               c = face((c0 >> 2) & 3u, ey, i, din, dout), dd = face((cd[ci - cy] >> 2) & 3u, ey, i - sy, din, dout),
+               f = face((c0 >> 4) & 3u, ez, i, din, dout), g = face((cd[ci - cz] >> 4) & 3u, ez, i - sz, din, dout);
         ns = (a * p[i + 1] + b * p[i - 1]) * ih + (c * p[i + sy] + dd * p[i - sy]) * ih +
              (f * p[i + sz] + g * p[i - sz]) * ih;
         dg = (a + b) * ih + (c + dd) * ih + (f + g) * ih + ((c0 & 64u) ? dkb : 0.0);
       }
       double q = (c0 & 128u) ? rho[i] : 0.0;
       double r = kFourPiEcB * q + ns - dg * p[i];
-      rhs0[i] = (float)r;
+      rhs0[ci] = (float)r;
       acc += r * r;
     }
   }
@@ -282,8 +285,9 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
 }
 
 // phi += e over every point (the prolongation can reach boundary points of
-// grids with even dimensions), then e = 0 for the next cycle; four points
-// per thread (phi and e start on 64-element boundaries).
+// grids with even dimensions), then e = 0 for the next cycle; 32 x 8 x 8
+// bricks, a warp reads 32 consecutive x of the padded FP32 row and of the
+// unpadded FP64 row.
 __global__ void __launch_bounds__(256) k_update64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
                                                   const JobState* __restrict__ S, int want) {
   int lb, j = wl_job(w, blockIdx.x, lb);
@@ -291,62 +295,254 @@ __global__ void __launch_bounds__(256) k_update64(WL w, const JobD* __restrict__
   const JobD& d = J[j];
   float* __restrict__ e0 = L[j * kMaxLev].e;
   double* __restrict__ phi = d.phi;
-  int n = d.nx * d.ny * d.nz;
-  int i = 4 * (lb * blockDim.x + threadIdx.x);
-  if (i + 3 < n) {
-    float4 e = *(const float4*)(e0 + i);
-    double2 a = *(const double2*)(phi + i), b = *(const double2*)(phi + i + 2);
-    a.x += (double)e.x;
-    a.y += (double)e.y;
-    b.x += (double)e.z;
-    b.y += (double)e.w;
-    *(double2*)(phi + i) = a;
-    *(double2*)(phi + i + 2) = b;
-    *(float4*)(e0 + i) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  } else {
-    for (int k = i; k < n; k++) {
-      phi[k] += (double)e0[k];
-      e0[k] = 0.0f;
-    }
+  int x, y, z0;
+  brick_col(lb, d.nx, d.ny, x, y, z0);
+  if (x >= d.nx || y >= d.ny) return;
+  const int sz = d.nx * d.ny, cz = d.px * d.ny;
+  int i = x + d.nx * y + sz * z0, ci = x + d.px * y + cz * z0;
+#pragma unroll
+  for (int k = 0; k < 8; k++, i += sz, ci += cz) {
+    if (z0 + k >= d.nz) break;
+    phi[i] += (double)e0[ci];
+    e0[ci] = 0.0f;
   }
 }
 
-// One colour of a red-black SOR sweep on one level (pb_solver.rs:250-317).
-// Thread k of a block row owns the colour's point (2t + parity, y) of the
-// (x, y) plane in kRbZ consecutive z planes.  Points of one colour do not
-// read each other, so all loads of the thread's points are issued before its
-// first store and are in flight together, and the job lookup and index
-// decode are paid once per kRbZ points (the pass is issue- and
-// latency-bound, not DRAM-bound, at one point per thread).
-constexpr int kRbZ = 4;
-__global__ void __launch_bounds__(256) k_rb32(WL w, const LvlD* __restrict__ L, int lvl,
-                                              const JobState* __restrict__ S, int colour) {
+// One full red-black sweep on one level (pb_solver.rs:250-317): every even
+// point (x + y + z even) from its odd neighbours, then every odd point from
+// the updated even ones, each point with the arithmetic of the
+// single-colour update.  A block owns an x-y tile of kSwTX x kSwTY points and
+// marches a chunk of z planes.  Planes of the correction (with a two-point
+// halo), of the right-hand side and of the stencil codes stream into
+// shared-memory rings with cp.async, two steps ahead of their use.  Step s
+// updates, in one phase between barriers, the even points of plane s+2 over
+// the tile and a one-point halo, the odd points of plane s (whose even
+// neighbours in planes s-1 .. s+1 are already updated) and writes plane s-1
+// out.  Halo values are recomputed by each tile that needs them, so the sweep
+// reads `src` and writes the whole grid, boundary values copied, into `dst`:
+// no block reads what another block writes.  Each thread's points, copy
+// chunks and store are fixed for the whole march (only the colour parity
+// alternates with the plane), so the per-step index work is a few adds; a
+// half-warp covers 16 points of one colour in a row and the next half-warp
+// the next row (opposite parity), so the shared loads are free of bank
+// conflicts; ring depths are powers of two.
+// z planes per block: long marches on the finest level, short ones on the
+// coarse levels (few tiles per grid there, so more chunks keep the SMs busy)
+constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 288;
+int sweep_chunk(int lvl) { return lvl == 0 ? 48 : 16; }
+constexpr int kSwW = kSwTX + 8;   // shared row: x in [xt-4, xt+TX+4), 16-byte chunks
+constexpr int kSwEY = kSwTY + 4;  // correction rows: y in [yt-2, yt+TY+2)
+constexpr int kSwRY = kSwTY + 2;  // right-hand-side rows: y in [yt-1, yt+TY+1)
+constexpr int kSwCY = kSwTY + 3;  // code rows: y in [yt-2, yt+TY+1)
+constexpr int kSwNE = 8, kSwNR = 8, kSwNC = 8;  // ring depths in planes (slot = plane & (depth - 1))
+// round 0: even points of plane s+2 inside the tile's x range, 16 per row, rows yt-1 .. yt+TY;
+// round 1: odd points of plane s (threads < TY*16), then the even points of plane s+2 on the
+// x halo (one per row: x = xt-1 or xt+TX)
+static_assert(kSwTX == 32 && (kSwTY + 2) * 16 == kSwThreads && kSwTY * 16 + kSwTY + 2 <= kSwThreads,
+              "point rounds of the sweep");
+static_assert(kSwEY * (kSwW / 4) <= kSwThreads && kSwRY * (kSwW / 4) <= kSwThreads &&
+                  kSwCY * (kSwW / 4) <= kSwThreads && kSwTY * (kSwTX / 4) <= kSwThreads,
+              "one copy chunk and one store per thread and plane");
+
+struct SwSmem {
+  float e[kSwNE][kSwEY * kSwW];
+  float r[kSwNR][kSwRY * kSwW];
+  uint8_t c[kSwNC][kSwCY * kSwW];
+};
+
+__device__ __forceinline__ void cp_async16(void* s, const void* g) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* s, const void* g) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(a), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Update of one interior point: off is its offset in the shared planes (the
+// right-hand-side planes start one row later), gi its padded global index
+// (for the map values of faces that cross the surface).
+__device__ __forceinline__ void sw_update(const Lv& d, float* __restrict__ E0, const float* __restrict__ Em,
+                                          const float* __restrict__ Ep, const float* __restrict__ R,
+                                          const uint8_t* __restrict__ C0, const uint8_t* __restrict__ Cm, int off,
+                                          int gi) {
+  float* ec = E0 + off;
+  const float xm = ec[-1], xp = ec[1], ym = ec[-kSwW], yp = ec[kSwW], zm = Em[off], zp = Ep[off], old = ec[0];
+  const float rhs = R[off - kSwW];
+  float ns, dg;
+  if (d.uni) {
+    ns = d.w6 * ((xp + xm) + (yp + ym) + (zp + zm));
+    dg = 6.0f * d.w6;
+  } else {
+    const unsigned c0 = C0[off], cxm = C0[off - 1], cym = C0[off - kSwW], czm = Cm[off];
+    float a, b, c, dd, f, g;
+    if (((c0 & 0x2Au) | (cxm & 0x2u) | (cym & 0x8u) | (czm & 0x20u)) == 0u) {  // no face crosses the surface
+      a = (c0 & 0x1u) ? d.fin : d.fout;
+      b = (cxm & 0x1u) ? d.fin : d.fout;
+      c = (c0 & 0x4u) ? d.fin : d.fout;
+      dd = (cym & 0x4u) ? d.fin : d.fout;
+      f = (c0 & 0x10u) ? d.fin : d.fout;
+      g = (czm & 0x10u) ? d.fin : d.fout;
+    } else {
+      a = face(c0 & 3u, d.ex, gi, d.fin, d.fout);
+      b = face(cxm & 3u, d.ex, gi - 1, d.fin, d.fout);
+      c = face((c0 >> 2) & 3u, d.ey, gi, d.fin, d.fout);
+      dd = face((cym >> 2) & 3u, d.ey, gi - d.sy, d.fin, d.fout);
+      f = face((c0 >> 4) & 3u, d.ez, gi, d.fin, d.fout);
+      g = face((czm >> 4) & 3u, d.ez, gi - d.sz, d.fin, d.fout);
+    }
+    ns = ((a * xp + b * xm) + (c * yp + dd * ym) + (f * zp + g * zm)) * d.ih;
+    dg = ((a + b) + (c + dd) + (f + g)) * d.ih + ((c0 & 64u) ? d.kb : 0.0f);
+  }
+  const float gs = __fdividef(ns + rhs, dg);
+  ec[0] = old + d.om * (gs - old);
+}
+
+__global__ void __launch_bounds__(kSwThreads, 4) k_sweep(WL w, const LvlD* __restrict__ L, int lvl,
+                                                      const JobState* __restrict__ S, int flip) {
+  extern __shared__ __align__(16) unsigned char sw_raw[];  // sizeof(SwSmem), above the 48 KB static limit
+  SwSmem& sm = *reinterpret_cast<SwSmem*>(sw_raw);
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != kMg) return;
   const Lv d = lv_load(L, j, lvl);
-  const int hw = (d.nx - 1) >> 1, plane = hw * (d.ny - 2);
-  const int nbp = (plane + kT - 1) / kT, bz = lb / nbp;
-  const int k = (lb - bz * nbp) * kT + threadIdx.x;
-  if (k >= plane) return;
-  const int t = k % hw, iy = 1 + k / hw, z0 = 1 + bz * kRbZ;
-  float ns[kRbZ], dg[kRbZ], ev[kRbZ], rv[kRbZ];
-  int idx[kRbZ];
-#pragma unroll
-  for (int r = 0; r < kRbZ; r++) {
-    const int z = z0 + r, ix = 1 + ((1 + iy + z + colour) & 1) + 2 * t;
-    idx[r] = (z <= d.nz - 2 && ix < d.nx - 1) ? ix + d.sy * iy + d.sz * z : -1;
-    if (idx[r] >= 0) {
-      st32(d, d.e, idx[r], ns[r], dg[r]);
-      ev[r] = d.e[idx[r]];
-      rv[r] = d.rhs[idx[r]];
+  const float* __restrict__ src = flip ? d.e2 : d.e;
+  float* __restrict__ dst = flip ? d.e : d.e2;
+  const int ntx = (d.nx + kSwTX - 1) / kSwTX, nty = (d.ny + kSwTY - 1) / kSwTY;
+  const int bx = lb % ntx, q = lb / ntx, by = q % nty, bz = q / nty;
+  const int xt = bx * kSwTX, yt = by * kSwTY;
+  const int z0 = bz * d.zc, z1 = min(z0 + d.zc, d.nz);
+  const int tid = threadIdx.x;
+
+  // copy chunks of this thread (shared offset, global offset within a plane; -1: none)
+  auto chunk = [&](int rows, int y0, int& so, int& go) {
+    so = go = -1;
+    if (tid >= rows * (kSwW / 4)) return;
+    const int r = tid / (kSwW / 4), c = tid % (kSwW / 4), y = y0 + r, x = xt - 4 + 4 * c;
+    if (y < 0 || y >= d.ny || x < 0 || x >= d.sy) return;
+    so = r * kSwW + 4 * c;
+    go = x + d.sy * y;
+  };
+  int eso, ego, rso, rgo, cso, cgo;
+  chunk(kSwEY, yt - 2, eso, ego);
+  chunk(kSwRY, yt - 1, rso, rgo);
+  chunk(kSwCY, yt - 2, cso, cgo);
+  if (d.uni) cso = -1;
+  // ring slot of plane p (p >= -2; two's complement & keeps negatives in range)
+  auto se_ = [](int p) { return p & (kSwNE - 1); };
+  auto sr_ = [](int p) { return p & (kSwNR - 1); };
+  auto sc_ = [](int p) { return p & (kSwNC - 1); };
+  auto load_e = [&](int p) {
+    if (ego >= 0 && p >= 0 && p < d.nz) cp_async16(&sm.e[se_(p)][eso], src + ego + (long long)d.sz * p);
+  };
+  auto load_r = [&](int p) {
+    if (rgo >= 0 && p >= 0 && p < d.nz) cp_async16(&sm.r[sr_(p)][rso], d.rhs + rgo + (long long)d.sz * p);
+  };
+  auto load_c = [&](int p) {
+    if (cso >= 0 && p >= 0 && p < d.nz) cp_async4(&sm.c[sc_(p)][cso], d.cd + cgo + (long long)d.sz * p);
+  };
+  // this thread's points.  Main (round 0): even point of row ym = yt-1+tid/16
+  // at x = xt + 2(tid%16) + ((xt + ym + p) & 1).  Round 1: odd point of row
+  // yo = yt + tid/16 at x = xt + 2(tid%16) + ((xt + yo + p + 1) & 1), or for
+  // threads TY*16 .. TY*16+TY+1 the halo even point of row yh = yt-1+(tid-TY*16)
+  // at xt-1 or xt+TX, whichever has the even colour.
+  const int cm = tid & 15;
+  const int ym = yt - 1 + (tid >> 4);
+  const bool m_ok = ym >= 1 && ym <= d.ny - 2;
+  const int m_pb = (xt + ym) & 1, m_off = (ym - yt + 2) * kSwW + 4 + 2 * cm, m_g = xt + 2 * cm + d.sy * ym;
+  int o_kind = 0, o_y = 0, o_pb = 0, o_off = 0, o_g = 0;  // 1 odd point, 2 halo even point
+  if (tid < kSwTY * 16) {
+    o_y = yt + (tid >> 4);
+    o_kind = 1;
+    o_pb = (xt + o_y + 1) & 1;
+    o_off = (o_y - yt + 2) * kSwW + 4 + 2 * cm;
+    o_g = xt + 2 * cm + d.sy * o_y;
+  } else if (tid < kSwTY * 16 + kSwTY + 2) {
+    o_y = yt - 1 + (tid - kSwTY * 16);
+    o_kind = 2;
+    o_pb = (xt - 1 + o_y) & 1;  // 0: x = xt-1 is even-coloured in even planes
+    o_off = (o_y - yt + 2) * kSwW + 3;
+    o_g = xt - 1 + d.sy * o_y;
+  }
+  if (o_y < 1 || o_y > d.ny - 2) o_kind = 0;
+  // store of this thread: one aligned float4 of a tile row
+  int sso = -1, sgo = 0;
+  if (tid < kSwTY * (kSwTX / 4)) {
+    const int r = tid / (kSwTX / 4), c = tid % (kSwTX / 4), y = yt + r, x = xt + 4 * c;
+    if (y < d.ny && x < d.sy) {
+      sso = (r + 2) * kSwW + 4 * c + 4;
+      sgo = x + d.sy * y;
     }
   }
-#pragma unroll
-  for (int r = 0; r < kRbZ; r++)
-    if (idx[r] >= 0) {
-      float gs = __fdividef(ns[r] + rv[r], dg[r]);
-      d.e[idx[r]] = ev[r] + d.om * (gs - ev[r]);
+  struct Planes {
+    float* E0;
+    const float *Em, *Ep, *R;
+    const uint8_t *C0, *Cm;
+    int gp;
+  };
+  auto planes = [&](int p) {
+    return Planes{sm.e[se_(p)], sm.e[se_(p - 1)], sm.e[se_(p + 1)], sm.r[sr_(p)],
+                  sm.c[sc_(p)], sm.c[sc_(p - 1)], d.sz * p};
+  };
+  auto update = [&](const Planes& P, int x, int off, int g) {
+    if (x >= 1 && x <= d.nx - 2) sw_update(d, P.E0, P.Em, P.Ep, P.R, P.C0, P.Cm, off, g + P.gp);
+  };
+  // even points of plane p: main round and halo
+  auto even = [&](int p) {
+    if (p < 1 || p > d.nz - 2) return;
+    const Planes P = planes(p);
+    const int par = m_pb ^ (p & 1);
+    if (m_ok) update(P, xt + 2 * cm + par, m_off + par, m_g + par);
+    if (o_kind == 2) {
+      const int h = (o_pb ^ (p & 1)) ? kSwTX + 1 : 0;  // xt-1 or xt+TX
+      update(P, xt - 1 + h, o_off + h, o_g + h);
     }
+  };
+  auto odd = [&](int p) {
+    if (o_kind != 1 || p < 1 || p > d.nz - 2) return;
+    const Planes P = planes(p);
+    const int par = o_pb ^ (p & 1);
+    update(P, xt + 2 * cm + par, o_off + par, o_g + par);
+  };
+  auto store = [&](int p) {
+    if (sso >= 0) *(float4*)(dst + sgo + (long long)d.sz * p) = *(const float4*)&sm.e[se_(p)][sso];
+  };
+
+  // prologue: what the even points of planes z0-1 .. z0+1 and step z0 read,
+  // then the planes of step z0+1
+  for (int p = z0 - 2; p <= z0 + 3; p++) load_e(p);
+  for (int p = z0 - 1; p <= z0 + 2; p++) load_r(p);
+  for (int p = z0 - 2; p <= z0 + 2; p++) load_c(p);
+  cp_async_commit();
+  load_e(z0 + 4);
+  load_r(z0 + 3);
+  load_c(z0 + 3);
+  cp_async_commit();
+  cp_async_wait<1>();
+  __syncthreads();
+  even(z0 - 1);
+  even(z0);
+  even(z0 + 1);
+  for (int s = z0; s < z1; s++) {
+    cp_async_wait<1>();  // all groups but the newest: correction planes to s+3, rhs / codes to s+2
+    __syncthreads();
+    if (s + 5 <= z1 + 1) load_e(s + 5);  // the last step reads correction planes to z1+1, rhs / codes to z1
+    if (s + 4 <= z1) {
+      load_r(s + 4);
+      load_c(s + 4);
+    }
+    cp_async_commit();
+    if (s + 2 <= z1) even(s + 2);
+    odd(s);
+    if (s > z0) store(s - 1);
+  }
+  __syncthreads();
+  store(z1 - 1);
+  cp_async_wait<0>();
 }
 
 // One colour of the plain SOR sweep (pb_solver.rs:373-447) on the level-0
@@ -411,6 +607,8 @@ __global__ void k_sor_norm(WL w, const JobD* __restrict__ J, JobState* __restric
     t.status = kSorCap;
 }
 
+// FP32 residual of the level's correction, which is in e2 after the three
+// pre-smoothing sweeps (e -> e2 -> e -> e2).
 __global__ void __launch_bounds__(256) k_res32(WL w, const LvlD* __restrict__ L, int lvl,
                                                const JobState* __restrict__ S) {
   int lb, j = wl_job(w, blockIdx.x, lb);
@@ -425,8 +623,8 @@ __global__ void __launch_bounds__(256) k_res32(WL w, const LvlD* __restrict__ L,
     if (z < 1 || z > d.nz - 2) continue;
     int i = x + d.sy * y + d.sz * z;
     float ns, dg;
-    st32(d, d.e, i, ns, dg);
-    d.res[i] = d.rhs[i] + ns - dg * d.e[i];
+    st32(d, d.e2, i, ns, dg);
+    d.res[i] = d.rhs[i] + ns - dg * d.e2[i];
   }
 }
 
@@ -472,7 +670,8 @@ __global__ void __launch_bounds__(256) k_restrict32(WL w, const LvlD* __restrict
 }
 
 // Trilinear prolongation of the level-(l+1) correction added at every
-// level-l point (pb_solver.rs:522-578).
+// level-l point (pb_solver.rs:522-578); the fine correction is in e2 between
+// the pre- and post-smoothing sweeps, the coarse one in e.
 __global__ void __launch_bounds__(256) k_prolong32(WL w, const LvlD* __restrict__ L, int lvl,
                                                    const JobState* __restrict__ S) {
   int lb, j = wl_job(w, blockIdx.x, lb);
@@ -497,7 +696,7 @@ __global__ void __launch_bounds__(256) k_prolong32(WL w, const LvlD* __restrict_
     float c01 = b[c.sz] * (1.0f - dx) + b[c.sz + 1] * dx;
     float c11 = b[c.sz + c.sy] * (1.0f - dx) + b[c.sz + c.sy + 1] * dx;
     float c0 = c00 * (1.0f - dy) + c10 * dy, c1 = c01 * (1.0f - dy) + c11 * dy;
-    f.e[fx + f.sy * fy + f.sz * fz] += c0 * (1.0f - dz) + c1 * dz;
+    f.e2[fx + f.sy * fy + f.sz * fz] += c0 * (1.0f - dz) + c1 * dz;
   }
 }
 
@@ -620,10 +819,11 @@ __global__ void k_maps32(WL w, const JobD* __restrict__ J, const LvlD* __restric
   int n = d.nx * d.ny * d.nz;
   int i = lb * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  ((float*)l0.ex)[i] = (float)d.ex[i];
-  ((float*)l0.ey)[i] = (float)d.ey[i];
-  ((float*)l0.ez)[i] = (float)d.ez[i];
-  ((float*)l0.k2)[i] = (float)d.k2[i];
+  const long long ci = i % d.nx + (long long)d.px * (i / d.nx);  // padded FP32 index
+  ((float*)l0.ex)[ci] = (float)d.ex[i];
+  ((float*)l0.ey)[ci] = (float)d.ey[i];
+  ((float*)l0.ez)[ci] = (float)d.ez[i];
+  ((float*)l0.k2)[ci] = (float)d.k2[i];
 }
 
 // Level-0 stencil codes of every grid from its FP64 maps (exact compares),
@@ -641,6 +841,8 @@ __global__ void k_codes(WL w, const JobD* __restrict__ J, const LvlD* __restrict
   int i = lb * blockDim.x + threadIdx.x;
   unsigned exc = 0, chg = 0;
   if (i < n) {
+    const int x = i % d.nx, t = i / d.nx;
+    const long long ci = x + (long long)d.px * t;  // t = y + ny z
     unsigned c = 0;
     if (!d.uniform) {
       unsigned a = fcode(d.ex[i], d.din, d.dout), b = fcode(d.ey[i], d.din, d.dout), e = fcode(d.ez[i], d.din, d.dout);
@@ -658,7 +860,7 @@ __global__ void k_codes(WL w, const JobD* __restrict__ J, const LvlD* __restrict
       c |= 128u;
       chg = 1;
     }
-    ((uint8_t*)L[j * kMaxLev].cd)[i] = (uint8_t)c;
+    ((uint8_t*)L[j * kMaxLev].cd)[ci] = (uint8_t)c;
   }
   exc = __reduce_add_sync(0xffffffffu, exc);
   chg = __reduce_add_sync(0xffffffffu, chg);
@@ -676,12 +878,13 @@ __global__ void k_inject32(WL w, const LvlD* __restrict__ L, int lvl) {
   int i = lb * blockDim.x + threadIdx.x;
   if (i >= cn) return;
   int cx = i % c.nx, cy = (i / c.nx) % c.ny, cz = i / (c.nx * c.ny);
-  int fi = min(2 * cx, f.nx - 1) + f.nx * (min(2 * cy, f.ny - 1) + f.ny * min(2 * cz, f.nz - 1));
-  ((float*)c.ex)[i] = f.ex[fi];
-  ((float*)c.ey)[i] = f.ey[fi];
-  ((float*)c.ez)[i] = f.ez[fi];
-  ((float*)c.k2)[i] = f.k2[fi];
-  ((uint8_t*)c.cd)[i] = f.cd[fi] & 127u;  // maps are injected, so are their codes; no rho below level 0
+  int fi = min(2 * cx, f.nx - 1) + f.px * (min(2 * cy, f.ny - 1) + f.ny * min(2 * cz, f.nz - 1));
+  int ci = cx + c.px * (cy + c.ny * cz);
+  ((float*)c.ex)[ci] = f.ex[fi];
+  ((float*)c.ey)[ci] = f.ey[fi];
+  ((float*)c.ez)[ci] = f.ez[fi];
+  ((float*)c.k2)[ci] = f.k2[fi];
+  ((uint8_t*)c.cd)[ci] = f.cd[fi] & 127u;  // maps are injected, so are their codes; no rho below level 0
 }
 
 // 0.5 sum_a q_a phi(x_a), trilinear phi (pb_solver.rs:1174-1186); one block per grid.
@@ -733,6 +936,10 @@ __global__ void k_maxabs64(const JobD* __restrict__ J, double* __restrict__ M) {
 }
 
 long long cdiv(long long n, int t) { return (n + t - 1) / t; }
+// FP32 and code arrays: rows padded to a multiple of 4 points (16 bytes of FP32)
+int pitch(const PbGeom& g) { return (int)((g.nx + 3) & ~3); }
+size_t padded_n(const PbGeom& g) { return (size_t)pitch(g) * g.ny * g.nz; }
+
 long long nbricks(const PbGeom& g) { return cdiv(g.nx, 32) * cdiv(g.ny, 8) * cdiv(g.nz, 8); }
 
 // Host-side work lists: per launch slot the listed grids and their first
@@ -833,8 +1040,8 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     Y.nlev = nl;
     for (int l = 0; l <= std::max(nl, 0); l++) {
       Y.o32[l] = n32;
-      size_t m = Y.lv[l].n();
-      n32 += (J.uniform ? 3 : 7) * m;
+      size_t m = padded_n(Y.lv[l]);
+      n32 += (J.uniform ? 4 : 8) * m;
       n32 = (n32 + 63) & ~(size_t)63;
       if (l == 0 || !J.uniform) {  // codes: rho bits of every level-0 grid, stencils of solvated grids
         Y.o8[l] = n8;
@@ -925,6 +1132,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       d.k2 = base + 5 * n;
     }
     d.cd = P8 + Y.o8[0];
+    d.px = pitch(J.g);
     d.din = J.ein;
     d.dout = J.eout;
     d.dkb = J.ionic ? p.solvent_dielectric * J.kap * J.kap : 0.0;  // assign_kappa, pb_grid.rs:964
@@ -956,18 +1164,21 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     max_sor = std::max(max_sor, cdiv((long long)((J.g.nx - 1) / 2) * (J.g.ny - 2) * (J.g.nz - 2), kT));
     for (int l = 0; l <= std::max(Y.nlev, 0); l++) {
       const PbGeom& g = Y.lv[l];
-      size_t m = g.n();
+      size_t m = padded_n(g);
       LvlD& L = hl[(size_t)j * kMaxLev + l];
       std::memset(&L, 0, sizeof(L));
       float* b = P32 + Y.o32[l];
       L.e = b;
-      L.rhs = b + m;
-      L.res = b + 2 * m;
+      L.e2 = b + m;
+      L.rhs = b + 2 * m;
+      L.res = b + 3 * m;
+      L.px = pitch(g);
+      L.zc = sweep_chunk(l);
       if (!J.uniform) {
-        L.ex = b + 3 * m;
-        L.ey = b + 4 * m;
-        L.ez = b + 5 * m;
-        L.k2 = b + 6 * m;
+        L.ex = b + 4 * m;
+        L.ey = b + 5 * m;
+        L.ez = b + 6 * m;
+        L.k2 = b + 7 * m;
         L.cd = P8 + Y.o8[l];
       } else if (l == 0) {
         L.cd = P8 + Y.o8[0];
@@ -1060,6 +1271,8 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     }
   }
   const int K = std::max(1, chunk_cycles), KS = 4;  // cycles per chunk, SOR sweeps per cycle
+  // the sweep's rings exceed the 48 KB default (set per call: the attribute is per device)
+  RSTG_CUDA(cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SwSmem)));
   bool use_graph = !profile && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
   std::vector<int> key;  // (job, status) pairs of the current lists
   std::vector<WL> wl;
@@ -1103,19 +1316,19 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   auto enqueue_chunk = [&]() {
     int n = 0;
     auto go = [&](int slot) { return lists.slots[slot].total; };
-    auto sweeps = [&](int l) {
-      for (int s = 0; s < 3; s++)
-        for (int colour = 0; colour < 2; colour++) {
-          mark(l == 0 ? 0 : -1, dSweep, l,
-               [&] { k_rb32<<<go(ls[l].rb), kT, 0, st>>>(wl[ls[l].rb], dL, l, dS, colour); });
-          n++;
-        }
+    // three sweeps: pre-smoothing e -> e2 -> e -> e2, post-smoothing back to e
+    auto sweeps = [&](int l, int first) {
+      for (int s = 0; s < 3; s++) {
+        const int flip = first ^ (s & 1);
+        mark(l == 0 ? 0 : -1, dSweep, l, [&] { k_sweep<<<go(ls[l].rb), kSwThreads, sizeof(SwSmem), st>>>(wl[ls[l].rb], dL, l, dS, flip); });
+        n++;
+      }
     };
     for (int k = 0; k < K; k++) {
       if (any_mg) {
         for (int l = 0; l <= maxlev; l++) {
           if (go(ls[l].rb)) {
-            sweeps(l);
+            sweeps(l, 0);
             mark(l == 0 ? 1 : -1, dRes32, l, [&] { k_res32<<<go(ls[l].res), kT, 0, st>>>(wl[ls[l].res], dL, l, dS); });
             mark(-1, dRestrict, l,
                  [&] { k_restrict32<<<go(ls[l].restr), kT, 0, st>>>(wl[ls[l].restr], dL, l, dS); });
@@ -1131,7 +1344,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           if (!go(ls[l].prol)) continue;
           mark(-1, dProlong, l, [&] { k_prolong32<<<go(ls[l].prol), kT, 0, st>>>(wl[ls[l].prol], dL, l, dS); });
           n++;
-          sweeps(l);
+          sweeps(l, 1);
         }
         mark(3, dUpdate, 0, [&] { k_update64<<<go(s_upd), kT, 0, st>>>(wl[s_upd], dJ, dL, dS, kMg); });
         mark(2, dRes64, 0, [&] { k_res64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, kMg, part, nparts); });
@@ -1178,20 +1391,20 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
         maxlev = std::max(maxlev, Y.nlev);
         for (int l = 0; l < Y.nlev; l++) {
           const PbGeom& a = Y.lv[l];
-          lists.add(ls[l].rb, j, cdiv((long long)((a.nx - 1) / 2) * (a.ny - 2), kT) * cdiv(a.nz - 2, kRbZ));
+          lists.add(ls[l].rb, j, cdiv(a.nx, kSwTX) * cdiv(a.ny, kSwTY) * cdiv(a.nz, sweep_chunk(l)));
           lists.add(ls[l].res, j, nbricks(a));
           lists.add(ls[l].restr, j, nbricks(Y.lv[l + 1]));
           lists.add(ls[l].prol, j, nbricks(a));
         }
         lists.add(ls[Y.nlev].coarse, j, 1);
-        lists.add(s_upd, j, cdiv(cdiv((long long)g.n(), 4), kT));
+        lists.add(s_upd, j, nbricks(g));
         lists.add(s_res, j, nbricks(g));
         lists.add(s_norm, j, 1);
       } else if (hs[j].status == kSor) {
         any_sor = true;
         lists.add(s_sres, j, nbricks(g));
         lists.add(s_sor, j, cdiv((long long)((g.nx - 1) / 2) * (g.ny - 2) * (g.nz - 2), kT));
-        lists.add(s_supd, j, cdiv(cdiv((long long)g.n(), 4), kT));
+        lists.add(s_supd, j, nbricks(g));
         lists.add(s_snorm, j, 1);
       }
     }
@@ -1200,7 +1413,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       if (hs[j].status == kMg) {
         double pts = (double)jobs[j].g.n(), exc = (double)counts[2 * j], chg = (double)counts[2 * j + 1];
         bool u = jobs[j].uniform;
-        kbytes[0] += pts * (u ? 10.0 : 11.0) + 4.0 * exc;  // e, rhs, (codes), half of e written; map reads
+        kbytes[0] += pts * (u ? 12.0 : 13.0) + 4.0 * exc;  // one sweep: e read and written, rhs, (codes); map reads
         kbytes[1] += pts * (u ? 12.0 : 13.0) + 4.0 * exc;  // e, rhs, (codes), res written; map reads
         kbytes[2] += pts * 13.0 + 8.0 * (exc + chg);        // phi, codes, rhs written; map and rho reads
         kbytes[3] += pts * 24.0;                            // phi and e read and written
