@@ -67,7 +67,7 @@ constexpr int kT = 256;
 constexpr int kMg = 0, kConverged = 1, kDiverged = 2, kMgCap = 3, kSor = 5, kSorCap = 6;
 
 struct JobD {
-  double* phi;
+  double *phi, *phi2;  // potential: two buffers, JobState::cur says which one is current
   const double* rho;
   const double *ex, *ey, *ez, *k2;
   const uint8_t* cd;      // level-0 stencil codes
@@ -92,7 +92,7 @@ struct LvlD {
 
 struct JobState {
   double best, prev, rms, r0, om;
-  int growing, cycles, status, pad;
+  int growing, cycles, status, cur;  // cur: phi2 holds the current potential
   long long sor_it;
 };
 
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__
   if (S[j].status != want) return;
   const JobD& d = J[j];
   float* __restrict__ rhs0 = L[j * kMaxLev].rhs;
-  const double* __restrict__ p = d.phi;
+  const double* __restrict__ p = S[j].cur ? d.phi2 : d.phi;
   const double* __restrict__ rho = d.rho;
   const double *__restrict__ ex = d.ex, *__restrict__ ey = d.ey, *__restrict__ ez = d.ez;
   const uint8_t* __restrict__ cd = d.cd;
@@ -243,6 +243,70 @@ __global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__
   if (threadIdx.x == 0) part[(long long)j * nparts + lb] = t;
 }
 
+// End of a V-cycle: phi' = phi + e at every point (the prolongation can
+// reach boundary points of grids with even dimensions) into the other
+// potential buffer, and the FP64 residual of phi' at the interior points, from
+// phi + e at the seven stencil points (the same values the separate update
+// would store), rounded to FP32 as the next right-hand side, squares summed
+// per brick.  The correction is not cleared: the next cycle's first sweep
+// reads it as zero.
+__global__ void __launch_bounds__(256, 3) k_upres64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
+                                                    const JobState* __restrict__ S, double* __restrict__ part,
+                                                    int nparts) {
+  __shared__ double sh[32];
+  int lb, j = wl_job(w, blockIdx.x, lb);
+  if (S[j].status != kMg) return;
+  const JobD& d = J[j];
+  const bool cur = S[j].cur != 0;
+  const double* __restrict__ p = cur ? d.phi2 : d.phi;
+  double* __restrict__ q = cur ? d.phi : d.phi2;
+  const float* __restrict__ e0 = L[j * kMaxLev].e;
+  float* __restrict__ rhs0 = L[j * kMaxLev].rhs;
+  const double* __restrict__ rho = d.rho;
+  const double *__restrict__ ex = d.ex, *__restrict__ ey = d.ey, *__restrict__ ez = d.ez;
+  const uint8_t* __restrict__ cd = d.cd;
+  const double din = d.din, dout = d.dout, dkb = d.dkb;
+  const bool uni = d.uniform != 0;
+  const double ih = d.ih, wt = d.eps * d.ih;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny;
+  int x, y, z0;
+  brick_col(lb, nx, ny, x, y, z0);
+  double acc = 0.0;
+  if (x < nx && y < ny) {
+    const bool inxy = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
+    int i = x + sy * y + sz * z0, ci = x + cy * y + cz * z0;  // FP64 and padded FP32 / code indices
+#pragma unroll 1
+    for (int k = 0; k < 8; k++, i += sz, ci += cz) {
+      const int z = z0 + k;
+      if (z >= nz) break;
+      const double v = p[i] + (double)e0[ci];
+      q[i] = v;
+      if (!inxy || z < 1 || z > nz - 2) continue;
+      const double vxp = p[i + 1] + (double)e0[ci + 1], vxm = p[i - 1] + (double)e0[ci - 1],
+                   vyp = p[i + sy] + (double)e0[ci + cy], vym = p[i - sy] + (double)e0[ci - cy],
+                   vzp = p[i + sz] + (double)e0[ci + cz], vzm = p[i - sz] + (double)e0[ci - cz];
+      const unsigned c0 = cd[ci];
+      double ns, dg;
+      if (uni) {
+        ns = wt * ((vxp + vxm) + (vyp + vym) + (vzp + vzm));
+        dg = 6.0 * wt;
+      } else {
+        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci - 1] & 3u, ex, i - 1, din, dout),
+               c = face((c0 >> 2) & 3u, ey, i, din, dout), dd = face((cd[ci - cy] >> 2) & 3u, ey, i - sy, din, dout),
+               f = face((c0 >> 4) & 3u, ez, i, din, dout), g = face((cd[ci - cz] >> 4) & 3u, ez, i - sz, din, dout);
+        ns = (a * vxp + b * vxm) * ih + (c * vyp + dd * vym) * ih + (f * vzp + g * vzm) * ih;
+        dg = (a + b) * ih + (c + dd) * ih + (f + g) * ih + ((c0 & 64u) ? dkb : 0.0);
+      }
+      double rq = (c0 & 128u) ? rho[i] : 0.0;
+      double r = kFourPiEcB * rq + ns - dg * v;
+      rhs0[ci] = (float)r;
+      acc += r * r;
+    }
+  }
+  double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[(long long)j * nparts + lb] = t;
+}
+
 // RMS of the residual and the reference's multigrid bookkeeping
 // (pb_solver.rs:1080-1160); one block per listed grid.
 __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ S, const double* __restrict__ part,
@@ -264,6 +328,7 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
     t.r0 = r;
     return;
   }
+  t.cur ^= 1;  // k_upres64 wrote the new potential into the other buffer
   t.cycles++;
   if (r < t.best) {
     t.best = r;
@@ -284,8 +349,7 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
   }
 }
 
-// phi += e over every point (the prolongation can reach boundary points of
-// grids with even dimensions), then e = 0 for the next cycle; 32 x 8 x 8
+// SOR fallback: phi += e over every point, then e = 0 for the next sweep; 32 x 8 x 8
 // bricks, a warp reads 32 consecutive x of the padded FP32 row and of the
 // unpadded FP64 row.
 __global__ void __launch_bounds__(256) k_update64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
@@ -294,7 +358,7 @@ __global__ void __launch_bounds__(256) k_update64(WL w, const JobD* __restrict__
   if (S[j].status != want) return;
   const JobD& d = J[j];
   float* __restrict__ e0 = L[j * kMaxLev].e;
-  double* __restrict__ phi = d.phi;
+  double* __restrict__ phi = S[j].cur ? d.phi2 : d.phi;
   int x, y, z0;
   brick_col(lb, d.nx, d.ny, x, y, z0);
   if (x >= d.nx || y >= d.ny) return;
@@ -404,7 +468,7 @@ __device__ __forceinline__ void sw_update(const Lv& d, float* __restrict__ E0, c
 }
 
 __global__ void __launch_bounds__(kSwThreads, 4) k_sweep(WL w, const LvlD* __restrict__ L, int lvl,
-                                                      const JobState* __restrict__ S, int flip) {
+                                                      const JobState* __restrict__ S, int flip, int zero_src) {
   extern __shared__ __align__(16) unsigned char sw_raw[];  // sizeof(SwSmem), above the 48 KB static limit
   SwSmem& sm = *reinterpret_cast<SwSmem*>(sw_raw);
   int lb, j = wl_job(w, blockIdx.x, lb);
@@ -436,8 +500,12 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep(WL w, const LvlD* __res
   auto se_ = [](int p) { return p & (kSwNE - 1); };
   auto sr_ = [](int p) { return p & (kSwNR - 1); };
   auto sc_ = [](int p) { return p & (kSwNC - 1); };
-  auto load_e = [&](int p) {
-    if (ego >= 0 && p >= 0 && p < d.nz) cp_async16(&sm.e[se_(p)][eso], src + ego + (long long)d.sz * p);
+  auto load_e = [&](int p) {  // zero_src: the correction is zero (first sweep of a cycle on the finest level)
+    if (ego < 0 || p < 0 || p >= d.nz) return;
+    if (zero_src)
+      *(float4*)&sm.e[se_(p)][eso] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    else
+      cp_async16(&sm.e[se_(p)][eso], src + ego + (long long)d.sz * p);
   };
   auto load_r = [&](int p) {
     if (rgo >= 0 && p >= 0 && p < d.nz) cp_async16(&sm.r[sr_(p)][rso], d.rhs + rgo + (long long)d.sz * p);
@@ -1018,7 +1086,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     Lay& Y = lay[j];
     size_t n = J.g.n();
     Y.o64 = n64;
-    n64 += (J.uniform ? 2 : 6) * n;
+    n64 += (J.uniform ? 3 : 7) * n;  // phi, rho, (4 maps), phi2
     n64 = (n64 + 63) & ~(size_t)63;
     PbGeom g = J.g;
     Y.lv[0] = g;
@@ -1071,6 +1139,8 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     RSTG_CUDA(cudaMemsetAsync(phi, 0, n * 8, st));
     if (J.bc.kind != 1) pb_boundary(c_, J.g, phi, *J.atoms, J.bc);
   }
+  std::vector<double*> phi_now(nj);  // current potential buffer of each grid (host view)
+  for (int j = 0; j < nj; j++) phi_now[j] = P64 + lay[j].o64;
   // Debye-Hueckel boundary values of the listed grids in one launch
   auto dh_launch = [&](const std::vector<int>& which) {
     std::vector<DhD> dd;
@@ -1079,7 +1149,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     for (int j : which) {
       const PbJob& J = jobs[j];
       DhD x;
-      x.phi = P64 + lay[j].o64;
+      x.phi = phi_now[j];
       x.xyz = J.atoms->xyz.as<double>();
       x.q = J.atoms->q.as<double>();
       x.nx = J.g.nx;
@@ -1124,6 +1194,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     JobD& d = hd[j];
     std::memset(&d, 0, sizeof(d));
     d.phi = base;
+    d.phi2 = base + (J.uniform ? 2 : 6) * n;
     d.rho = base + n;
     if (!J.uniform) {
       d.ex = base + 2 * n;
@@ -1283,7 +1354,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     int rb, res, restr, coarse, prol;
   };
   std::vector<LvSlots> ls(kMaxLev);
-  int s_upd = 0, s_res = 0, s_norm = 0, s_sres = 0, s_sor = 0, s_supd = 0, s_snorm = 0, maxlev = 0;
+  int s_res = 0, s_norm = 0, s_sres = 0, s_sor = 0, s_supd = 0, s_snorm = 0, maxlev = 0;
   bool any_mg = false, any_sor = false;
   // profile mode: events around every launch; the level-0 kernels also
   // carry their algorithmic bytes (compulsory DRAM traffic per launch) from
@@ -1317,10 +1388,13 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     int n = 0;
     auto go = [&](int slot) { return lists.slots[slot].total; };
     // three sweeps: pre-smoothing e -> e2 -> e -> e2, post-smoothing back to e
+    // (the finest level's correction is not cleared between cycles: its first sweep reads zeros)
     auto sweeps = [&](int l, int first) {
       for (int s = 0; s < 3; s++) {
-        const int flip = first ^ (s & 1);
-        mark(l == 0 ? 0 : -1, dSweep, l, [&] { k_sweep<<<go(ls[l].rb), kSwThreads, sizeof(SwSmem), st>>>(wl[ls[l].rb], dL, l, dS, flip); });
+        const int flip = first ^ (s & 1), zero = (l == 0 && first == 0 && s == 0) ? 1 : 0;
+        mark(l == 0 ? 0 : -1, dSweep, l, [&] {
+          k_sweep<<<go(ls[l].rb), kSwThreads, sizeof(SwSmem), st>>>(wl[ls[l].rb], dL, l, dS, flip, zero);
+        });
         n++;
       }
     };
@@ -1346,8 +1420,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           n++;
           sweeps(l, 1);
         }
-        mark(3, dUpdate, 0, [&] { k_update64<<<go(s_upd), kT, 0, st>>>(wl[s_upd], dJ, dL, dS, kMg); });
-        mark(2, dRes64, 0, [&] { k_res64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, kMg, part, nparts); });
+        mark(2, dRes64, 0, [&] { k_upres64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, part, nparts); });
         mark(-1, dNorm, 0, [&] { k_norm<<<go(s_norm), 256, 0, st>>>(wl[s_norm], dJ, dS, part, nparts, 1); });
         n += 3;
       }
@@ -1375,7 +1448,6 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     maxlev = 0;
     for (int l = 0; l < kMaxLev; l++)
       ls[l] = LvSlots{lists.add_slot(), lists.add_slot(), lists.add_slot(), lists.add_slot(), lists.add_slot()};
-    s_upd = lists.add_slot();
     s_res = lists.add_slot();
     s_norm = lists.add_slot();
     s_sres = lists.add_slot();
@@ -1397,7 +1469,6 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           lists.add(ls[l].prol, j, nbricks(a));
         }
         lists.add(ls[Y.nlev].coarse, j, 1);
-        lists.add(s_upd, j, nbricks(g));
         lists.add(s_res, j, nbricks(g));
         lists.add(s_norm, j, 1);
       } else if (hs[j].status == kSor) {
@@ -1415,8 +1486,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
         bool u = jobs[j].uniform;
         kbytes[0] += pts * (u ? 12.0 : 13.0) + 4.0 * exc;  // one sweep: e read and written, rhs, (codes); map reads
         kbytes[1] += pts * (u ? 12.0 : 13.0) + 4.0 * exc;  // e, rhs, (codes), res written; map reads
-        kbytes[2] += pts * 13.0 + 8.0 * (exc + chg);        // phi, codes, rhs written; map and rho reads
-        kbytes[3] += pts * 24.0;                            // phi and e read and written
+        kbytes[2] += pts * 25.0 + 8.0 * (exc + chg);  // phi and e read, phi' and rhs written, codes; map, rho reads
       }
     lists.upload(lists_, st, wl);
     if (use_graph && (any_mg || any_sor)) {
@@ -1441,10 +1511,13 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     std::vector<int> redo;
     for (int j = 0; j < nj; j++)
       if (hs[j].status == kDiverged) {
+        phi_now[j] = hs[j].cur ? hd[j].phi2 : hd[j].phi;
         if (jobs[j].bc.kind == 1)
           redo.push_back(j);
         else
-          pb_boundary(c_, jobs[j].g, hd[j].phi, *jobs[j].atoms, jobs[j].bc);
+          pb_boundary(c_, jobs[j].g, phi_now[j], *jobs[j].atoms, jobs[j].bc);
+        // SOR sweeps start from e = 0 (the V-cycles leave their last correction)
+        RSTG_CUDA(cudaMemsetAsync(hl[(size_t)j * kMaxLev].e, 0, padded_n(jobs[j].g) * 4, st));
         hs[j].status = kSor;
         hs[j].om = 1.0;
         hs[j].sor_it = 0;
@@ -1517,6 +1590,11 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     if (sor) stats.fallbacks++;
     jobs[j].stats = PbSolveStats{sor ? (int64_t)s.sor_it : (int64_t)s.cycles, s.rms, s.status == kConverged};
   }
+  for (int j = 0; j < nj; j++) {  // the energy kernels read JobD::phi: point it at the current buffer
+    phi_now[j] = hs[j].cur ? hd[j].phi2 : hd[j].phi;
+    hd[j].phi = phi_now[j];
+  }
+  RSTG_CUDA(cudaMemcpyAsync(dJ, hd.data(), sizeof(JobD) * nj, cudaMemcpyHostToDevice, st));
   double* dE = small_.as<double>();
   double* dM = dE + nj;
   k_energy64<<<nj, 256, 0, st>>>(dJ, dE);
@@ -1527,7 +1605,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   if (phi_out)
     for (int j = 0; j < nj; j++)
       if ((*phi_out)[j])
-        RSTG_CUDA(cudaMemcpyAsync((*phi_out)[j], P64 + lay[j].o64, jobs[j].g.n() * 8, cudaMemcpyDeviceToDevice, st));
+        RSTG_CUDA(cudaMemcpyAsync((*phi_out)[j], phi_now[j], jobs[j].g.n() * 8, cudaMemcpyDeviceToDevice, st));
   RSTG_CUDA(cudaStreamSynchronize(st));
   for (int j = 0; j < nj; j++) {
     jobs[j].e = he[j];
