@@ -928,9 +928,9 @@ int64_t System::pb_points_estimate() const {
 int64_t System::footprint(int64_t F) const {
   if (opts.mode == RSTG_MODE_PLAIN) return nC * 200 + F * 0;
   int64_t pb = 0;
-  if (solv.method == 1) {  // PB pools: ~80 B per solvated and ~30 B per reference grid point
+  if (solv.method == 1) {  // PB pools: ~95 B per solvated and ~45 B per reference grid point
     int64_t fpb = pb_frames_per_batch > 0 ? std::min(F, pb_frames_per_batch) : std::min<int64_t>(F, 16);
-    pb = fpb * pb_points_estimate() * 112;
+    pb = fpb * pb_points_estimate() * 140;
   }
   int64_t per = n_top * 24 + nC * (24 + 16 + 16 + 4 + 8 + 8 + 4 + (int64_t)nbr_cap * 4 + 16) + nR * 24 + nL * 16 +
                 (n_res_rec + n_res_lig) * 32 + 256;
@@ -1422,7 +1422,7 @@ void System::run_pb(const void* frames, bool f64, bool host_in, int64_t F, rstg_
     size_t fr = 0, tot = 0;
     RSTG_CUDA(cudaMemGetInfo(&fr, &tot));
     double budget = std::min(0.6 * (double)fr, 24e9);
-    chunk = std::max<int64_t>(1, (int64_t)(budget / (112.0 * (double)std::max<int64_t>(pb_points_estimate(), 1))));
+    chunk = std::max<int64_t>(1, (int64_t)(budget / (140.0 * (double)std::max<int64_t>(pb_points_estimate(), 1))));
   }
   std::vector<std::vector<double>> xs;
   std::vector<double> pol;
