@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__
   if (threadIdx.x == 0) part[(long long)j * nparts + lb] = t;
 }
 
-// End of a V-cycle: phi' = phi + e at every point (the prolongation can
+// End of a V-cycle (or of an SOR sweep): phi' = phi + e at every point (the prolongation can
 // reach boundary points of grids with even dimensions) into the other
 // potential buffer, and the FP64 residual of phi' at the interior points, from
 // phi + e at the seven stencil points (the same values the separate update
@@ -251,11 +251,11 @@ __global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__
 // per brick.  The correction is not cleared: the next cycle's first sweep
 // reads it as zero.
 __global__ void __launch_bounds__(256, 3) k_upres64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
-                                                    const JobState* __restrict__ S, double* __restrict__ part,
-                                                    int nparts) {
+                                                    const JobState* __restrict__ S, int want,
+                                                    double* __restrict__ part, int nparts) {
   __shared__ double sh[32];
   int lb, j = wl_job(w, blockIdx.x, lb);
-  if (S[j].status != kMg) return;
+  if (S[j].status != want) return;
   const JobD& d = J[j];
   const bool cur = S[j].cur != 0;
   const double* __restrict__ p = cur ? d.phi2 : d.phi;
@@ -349,29 +349,6 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
   }
 }
 
-// SOR fallback: phi += e over every point, then e = 0 for the next sweep; 32 x 8 x 8
-// bricks, a warp reads 32 consecutive x of the padded FP32 row and of the
-// unpadded FP64 row.
-__global__ void __launch_bounds__(256) k_update64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
-                                                  const JobState* __restrict__ S, int want) {
-  int lb, j = wl_job(w, blockIdx.x, lb);
-  if (S[j].status != want) return;
-  const JobD& d = J[j];
-  float* __restrict__ e0 = L[j * kMaxLev].e;
-  double* __restrict__ phi = S[j].cur ? d.phi2 : d.phi;
-  int x, y, z0;
-  brick_col(lb, d.nx, d.ny, x, y, z0);
-  if (x >= d.nx || y >= d.ny) return;
-  const int sz = d.nx * d.ny, cz = d.px * d.ny;
-  int i = x + d.nx * y + sz * z0, ci = x + d.px * y + cz * z0;
-#pragma unroll
-  for (int k = 0; k < 8; k++, i += sz, ci += cz) {
-    if (z0 + k >= d.nz) break;
-    phi[i] += (double)e0[ci];
-    e0[ci] = 0.0f;
-  }
-}
-
 // One full red-black sweep on one level (pb_solver.rs:250-317): every even
 // point (x + y + z even) from its odd neighbours, then every odd point from
 // the updated even ones, each point with the arithmetic of the
@@ -392,8 +369,8 @@ __global__ void __launch_bounds__(256) k_update64(WL w, const JobD* __restrict__
 // conflicts; ring depths are powers of two.
 // z planes per block: long marches on the finest level, short ones on the
 // coarse levels (few tiles per grid there, so more chunks keep the SMs busy)
-constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 288;
-int sweep_chunk(int lvl) { return lvl == 0 ? 48 : 16; }
+constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 288, kSwZC0 = 48, kSwZC1 = 16;
+int sweep_chunk(int lvl) { return lvl == 0 ? kSwZC0 : kSwZC1; }
 constexpr int kSwW = kSwTX + 8;   // shared row: x in [xt-4, xt+TX+4), 16-byte chunks
 constexpr int kSwEY = kSwTY + 4;  // correction rows: y in [yt-2, yt+TY+2)
 constexpr int kSwRY = kSwTY + 2;  // right-hand-side rows: y in [yt-1, yt+TY+1)
@@ -430,11 +407,14 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // Update of one interior point: off is its offset in the shared planes (the
 // right-hand-side planes start one row later), gi its padded global index
-// (for the map values of faces that cross the surface).
-__device__ __forceinline__ void sw_update(const Lv& d, float* __restrict__ E0, const float* __restrict__ Em,
-                                          const float* __restrict__ Ep, const float* __restrict__ R,
-                                          const uint8_t* __restrict__ C0, const uint8_t* __restrict__ Cm, int off,
-                                          int gi) {
+// (for the map values of faces that cross the surface).  Returns gs - old.
+// Multigrid smoothing divides with the fast reciprocal; the SOR fallback
+// (pb_solver.rs:373-447) with the exact division, as a plain sweep does.
+template <bool kExact>
+__device__ __forceinline__ float sw_update(const Lv& d, float om, float* __restrict__ E0,
+                                           const float* __restrict__ Em, const float* __restrict__ Ep,
+                                           const float* __restrict__ R, const uint8_t* __restrict__ C0,
+                                           const uint8_t* __restrict__ Cm, int off, int gi) {
   float* ec = E0 + off;
   const float xm = ec[-1], xp = ec[1], ym = ec[-kSwW], yp = ec[kSwW], zm = Em[off], zp = Ep[off], old = ec[0];
   const float rhs = R[off - kSwW];
@@ -463,17 +443,28 @@ __device__ __forceinline__ void sw_update(const Lv& d, float* __restrict__ E0, c
     ns = ((a * xp + b * xm) + (c * yp + dd * ym) + (f * zp + g * zm)) * d.ih;
     dg = ((a + b) + (c + dd) + (f + g)) * d.ih + ((c0 & 64u) ? d.kb : 0.0f);
   }
-  const float gs = __fdividef(ns + rhs, dg);
-  ec[0] = old + d.om * (gs - old);
+  const float gs = kExact ? (ns + rhs) / dg : __fdividef(ns + rhs, dg);
+  const float dv = gs - old;
+  ec[0] = old + om * dv;
+  return dv;
 }
 
-__global__ void __launch_bounds__(kSwThreads, 4) k_sweep(WL w, const LvlD* __restrict__ L, int lvl,
-                                                      const JobState* __restrict__ S, int flip, int zero_src) {
+// kSorMode: one sweep of the SOR fallback on the finest level's correction
+// equation from e = 0 (zero_src), with the grid's Chebyshev omega, and per
+// block the sum of (gs - old)^2 over the block's own points into
+// part[grid * nparts + block] (halo points are another block's).
+template <bool kSorMode>
+__global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __restrict__ L, int lvl,
+                                                        const JobState* __restrict__ S, int flip, int zero_src,
+                                                        double* __restrict__ part, int nparts) {
   extern __shared__ __align__(16) unsigned char sw_raw[];  // sizeof(SwSmem), above the 48 KB static limit
   SwSmem& sm = *reinterpret_cast<SwSmem*>(sw_raw);
+  __shared__ double red[32];
   int lb, j = wl_job(w, blockIdx.x, lb);
-  if (S[j].status != kMg) return;
+  if (S[j].status != (kSorMode ? kSor : kMg)) return;
   const Lv d = lv_load(L, j, lvl);
+  const float om = kSorMode ? (float)S[j].om : d.om;
+  double acc = 0.0;
   const float* __restrict__ src = flip ? d.e2 : d.e;
   float* __restrict__ dst = flip ? d.e : d.e2;
   const int ntx = (d.nx + kSwTX - 1) / kSwTX, nty = (d.ny + kSwTY - 1) / kSwTY;
@@ -556,25 +547,29 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep(WL w, const LvlD* __res
     return Planes{sm.e[se_(p)], sm.e[se_(p - 1)], sm.e[se_(p + 1)], sm.r[sr_(p)],
                   sm.c[sc_(p)], sm.c[sc_(p - 1)], d.sz * p};
   };
-  auto update = [&](const Planes& P, int x, int off, int g) {
-    if (x >= 1 && x <= d.nx - 2) sw_update(d, P.E0, P.Em, P.Ep, P.R, P.C0, P.Cm, off, g + P.gp);
+  auto update = [&](const Planes& P, int x, int off, int g, bool own) {
+    if (x < 1 || x > d.nx - 2) return;
+    const float dv = sw_update<kSorMode>(d, om, P.E0, P.Em, P.Ep, P.R, P.C0, P.Cm, off, g + P.gp);
+    if (kSorMode && own) acc += (double)dv * (double)dv;
   };
+  const bool m_own = ym >= yt && ym < yt + kSwTY;  // main-round row inside the tile (not the y halo)
   // even points of plane p: main round and halo
   auto even = [&](int p) {
     if (p < 1 || p > d.nz - 2) return;
     const Planes P = planes(p);
     const int par = m_pb ^ (p & 1);
-    if (m_ok) update(P, xt + 2 * cm + par, m_off + par, m_g + par);
+    const bool own = p >= z0 && p < z1;
+    if (m_ok) update(P, xt + 2 * cm + par, m_off + par, m_g + par, own && m_own);
     if (o_kind == 2) {
       const int h = (o_pb ^ (p & 1)) ? kSwTX + 1 : 0;  // xt-1 or xt+TX
-      update(P, xt - 1 + h, o_off + h, o_g + h);
+      update(P, xt - 1 + h, o_off + h, o_g + h, false);
     }
   };
   auto odd = [&](int p) {
     if (o_kind != 1 || p < 1 || p > d.nz - 2) return;
     const Planes P = planes(p);
     const int par = o_pb ^ (p & 1);
-    update(P, xt + 2 * cm + par, o_off + par, o_g + par);
+    update(P, xt + 2 * cm + par, o_off + par, o_g + par, true);
   };
   auto store = [&](int p) {
     if (sso >= 0) *(float4*)(dst + sgo + (long long)d.sz * p) = *(const float4*)&sm.e[se_(p)][sso];
@@ -611,59 +606,32 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep(WL w, const LvlD* __res
   __syncthreads();
   store(z1 - 1);
   cp_async_wait<0>();
-}
-
-// One colour of the plain SOR sweep (pb_solver.rs:373-447) on the level-0
-// correction, from e = 0, with per-block sums of (gs - old)^2.
-__global__ void k_sor32(WL w, const LvlD* __restrict__ L, const JobState* __restrict__ S, int colour,
-                        double* __restrict__ part, int nparts) {
-  __shared__ double sh[32];
-  int lb, j = wl_job(w, blockIdx.x, lb);
-  if (S[j].status != kSor) return;
-  const Lv d = lv_load(L, j, 0);
-  float om = (float)S[j].om;
-  int hw = (d.nx - 1) >> 1, nyi = d.ny - 2;
-  int cnt = hw * nyi * (d.nz - 2);
-  int k = lb * blockDim.x + threadIdx.x;
-  double acc = 0.0;
-  if (k < cnt) {
-    int t = k % hw, row = k / hw;
-    int iy = 1 + row % nyi, iz = 1 + row / nyi;
-    int ix = 1 + ((1 + iy + iz + colour) & 1) + 2 * t;
-    if (ix < d.nx - 1) {
-      int i = ix + d.sy * iy + d.sz * iz;
-      float ns, dg;
-      st32(d, d.e, i, ns, dg);
-      float old = d.e[i];
-      float gs = (ns + d.rhs[i]) / dg;
-      float dv = gs - old;
-      acc = (double)dv * (double)dv;
-      d.e[i] = old + om * dv;
-    }
+  if (kSorMode) {
+    const double t = block_sum(acc, red);
+    if (threadIdx.x == 0) part[(long long)j * nparts + lb] = t;
   }
-  double s = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[((long long)j * 2 + colour) * nparts + lb] = s;
 }
+#define k_sweep k_sweep_t<false>
+#define k_sor_sweep k_sweep_t<true>
 
-// SOR bookkeeping: rms of the sweep's updates, Chebyshev omega, convergence
-// (pb_solver.rs:373-447).
+// SOR bookkeeping after a sweep and its update (pb_solver.rs:373-447): rms
+// of the sweep's updates from the sweep blocks' partial sums (fixed order),
+// Chebyshev omega for the next sweep, convergence; k_upres64 wrote the new
+// potential into the other buffer.
 __global__ void k_sor_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ S, const double* __restrict__ part,
                            int nparts) {
   __shared__ double sh[32];
   int j = w.job[blockIdx.x];
   if (S[j].status != kSor) return;
   const JobD& d = J[j];
-  int used = (int)(((long long)((d.nx - 1) >> 1) * (d.ny - 2) * (d.nz - 2) + kT - 1) / kT);
+  const int used = ((d.nx + kSwTX - 1) / kSwTX) * ((d.ny + kSwTY - 1) / kSwTY) * ((d.nz + kSwZC0 - 1) / kSwZC0);
   double s = 0.0;
-  for (int c = 0; c < 2; c++) {  // per colour, then the two colour sums
-    double sc = 0.0;
-    for (int k = threadIdx.x; k < used; k += blockDim.x) sc += part[((long long)j * 2 + c) * nparts + k];
-    sc = block_sum(sc, sh);
-    s += sc;
-  }
+  for (int k = threadIdx.x; k < used; k += blockDim.x) s += part[(long long)j * nparts + k];
+  s = block_sum(s, sh);
   if (threadIdx.x != 0) return;
   double cnt = (double)(d.nx - 2) * (double)(d.ny - 2) * (double)(d.nz - 2);
   JobState& t = S[j];
+  t.cur ^= 1;
   double rms = cnt > 0.0 ? sqrt(s / cnt) : 0.0;
   long long it = t.sor_it;
   t.rms = rms;
@@ -1181,6 +1149,10 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     dh_launch(which);
   }
 
+  if (std::getenv("RSTG_PB_DEBUG")) {
+    RSTG_CUDA(cudaStreamSynchronize(st));
+    std::fprintf(stderr, "pb set-up: maps and boundary values of %d grids %.2f ms\n", nj, ms(t0, now()));
+  }
   // ---- descriptors ----------------------------------------------------------
   std::vector<JobD> hd(nj);
   std::vector<LvlD> hl((size_t)nj * kMaxLev);
@@ -1232,7 +1204,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     s.om = 1.0;
     s.status = Y.nlev >= 0 ? kMg : kSor;
     max_res = std::max(max_res, nbricks(J.g));
-    max_sor = std::max(max_sor, cdiv((long long)((J.g.nx - 1) / 2) * (J.g.ny - 2) * (J.g.nz - 2), kT));
+    max_sor = std::max(max_sor, cdiv(J.g.nx, kSwTX) * cdiv(J.g.ny, kSwTY) * cdiv(J.g.nz, kSwZC0));  // sweep blocks
     for (int l = 0; l <= std::max(Y.nlev, 0); l++) {
       const PbGeom& g = Y.lv[l];
       size_t m = padded_n(g);
@@ -1275,7 +1247,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   RSTG_CUDA(cudaMemcpyAsync(dJ, hd.data(), sizeof(JobD) * nj, cudaMemcpyHostToDevice, st));
   RSTG_CUDA(cudaMemcpyAsync(dL, hl.data(), sizeof(LvlD) * hl.size(), cudaMemcpyHostToDevice, st));
   RSTG_CUDA(cudaMemcpyAsync(dS, hs.data(), sizeof(JobState) * nj, cudaMemcpyHostToDevice, st));
-  size_t pbytes = (size_t)nparts * nj * 8 * 3;  // residual partials, then two colours of SOR partials
+  size_t pbytes = (size_t)nparts * nj * 8 * 2;  // residual partials, then SOR sweep partials
   if (part_.bytes < pbytes) part_ = DevBuf(pbytes, st);
   if (small_.bytes < (size_t)nj * 32 + 16) small_ = DevBuf((size_t)nj * 32 + 16, st);
   double* part = part_.as<double>();
@@ -1324,13 +1296,28 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   // ---- lock-step iterations ------------------------------------------------
   // Initial residuals of the multigrid grids (no convergence test: the
   // reference tests after each V-cycle).
+  // SOR grids (too small for multigrid) start from the residual of their
+  // initial potential as well.
+  auto sor_residuals = [&](const std::vector<int>& which) {
+    Lists rl;
+    int s = rl.add_slot();
+    for (int j : which) rl.add(s, j, nbricks(jobs[j].g));
+    if (rl.slots[s].total == 0) return;
+    std::vector<WL> wl;
+    rl.upload(lists_, st, wl);
+    k_res64<<<rl.slots[s].total, kT, 0, st>>>(wl[s], dJ, dL, dS, kSor, part, nparts);
+    launched(c_);
+  };
   {
     Lists init;
     int s = init.add_slot(), sn = init.add_slot();
+    std::vector<int> sor0;
     for (int j = 0; j < nj; j++)
       if (hs[j].status == kMg) {
         init.add(s, j, nbricks(jobs[j].g));
         init.add(sn, j, 1);
+      } else if (hs[j].status == kSor) {
+        sor0.push_back(j);
       }
     if (init.slots[s].total > 0) {
       std::vector<WL> wl;
@@ -1338,12 +1325,14 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       k_res64<<<init.slots[s].total, kT, 0, st>>>(wl[s], dJ, dL, dS, kMg, part, nparts);
       k_norm<<<init.slots[sn].total, 256, 0, st>>>(wl[sn], dJ, dS, part, nparts, 0);
       launched(c_, 2);
-      RSTG_CUDA(cudaStreamSynchronize(st));
     }
+    sor_residuals(sor0);
+    RSTG_CUDA(cudaStreamSynchronize(st));
   }
   const int K = std::max(1, chunk_cycles), KS = 4;  // cycles per chunk, SOR sweeps per cycle
   // the sweep's rings exceed the 48 KB default (set per call: the attribute is per device)
   RSTG_CUDA(cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SwSmem)));
+  RSTG_CUDA(cudaFuncSetAttribute(k_sor_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SwSmem)));
   bool use_graph = !profile && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
   std::vector<int> key;  // (job, status) pairs of the current lists
   std::vector<WL> wl;
@@ -1354,7 +1343,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     int rb, res, restr, coarse, prol;
   };
   std::vector<LvSlots> ls(kMaxLev);
-  int s_res = 0, s_norm = 0, s_sres = 0, s_sor = 0, s_supd = 0, s_snorm = 0, maxlev = 0;
+  int s_res = 0, s_norm = 0, s_sres = 0, s_sor = 0, s_snorm = 0, maxlev = 0;
   bool any_mg = false, any_sor = false;
   // profile mode: events around every launch; the level-0 kernels also
   // carry their algorithmic bytes (compulsory DRAM traffic per launch) from
@@ -1393,7 +1382,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       for (int s = 0; s < 3; s++) {
         const int flip = first ^ (s & 1), zero = (l == 0 && first == 0 && s == 0) ? 1 : 0;
         mark(l == 0 ? 0 : -1, dSweep, l, [&] {
-          k_sweep<<<go(ls[l].rb), kSwThreads, sizeof(SwSmem), st>>>(wl[ls[l].rb], dL, l, dS, flip, zero);
+          k_sweep<<<go(ls[l].rb), kSwThreads, sizeof(SwSmem), st>>>(wl[ls[l].rb], dL, l, dS, flip, zero, nullptr, 0);
         });
         n++;
       }
@@ -1420,20 +1409,20 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           n++;
           sweeps(l, 1);
         }
-        mark(2, dRes64, 0, [&] { k_upres64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, part, nparts); });
+        mark(2, dRes64, 0, [&] { k_upres64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, kMg, part, nparts); });
         mark(-1, dNorm, 0, [&] { k_norm<<<go(s_norm), 256, 0, st>>>(wl[s_norm], dJ, dS, part, nparts, 1); });
         n += 3;
       }
       if (any_sor)
         for (int q = 0; q < KS; q++) {
+          // sweep from e = 0 into e (the residual of the current potential is in rhs),
+          // phi' = phi + e with the next residual, bookkeeping
           mark(-1, dSor, 0, [&] {
-            k_res64<<<go(s_sres), kT, 0, st>>>(wl[s_sres], dJ, dL, dS, kSor, part, nparts);
-            k_sor32<<<go(s_sor), kT, 0, st>>>(wl[s_sor], dL, dS, 0, spart, nparts);
-            k_sor32<<<go(s_sor), kT, 0, st>>>(wl[s_sor], dL, dS, 1, spart, nparts);
-            k_update64<<<go(s_supd), kT, 0, st>>>(wl[s_supd], dJ, dL, dS, kSor);
+            k_sor_sweep<<<go(s_sor), kSwThreads, sizeof(SwSmem), st>>>(wl[s_sor], dL, 0, dS, 1, 1, spart, nparts);
+            k_upres64<<<go(s_sres), kT, 0, st>>>(wl[s_sres], dJ, dL, dS, kSor, part, nparts);
             k_sor_norm<<<go(s_snorm), 256, 0, st>>>(wl[s_snorm], dJ, dS, spart, nparts);
           });
-          n += 5;
+          n += 3;
         }
     }
     return n;
@@ -1452,7 +1441,6 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     s_norm = lists.add_slot();
     s_sres = lists.add_slot();
     s_sor = lists.add_slot();
-    s_supd = lists.add_slot();
     s_snorm = lists.add_slot();
     any_mg = any_sor = false;
     for (int j = 0; j < nj; j++) {
@@ -1474,8 +1462,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       } else if (hs[j].status == kSor) {
         any_sor = true;
         lists.add(s_sres, j, nbricks(g));
-        lists.add(s_sor, j, cdiv((long long)((g.nx - 1) / 2) * (g.ny - 2) * (g.nz - 2), kT));
-        lists.add(s_supd, j, nbricks(g));
+        lists.add(s_sor, j, cdiv(g.nx, kSwTX) * cdiv(g.ny, kSwTY) * cdiv(g.nz, kSwZC0));
         lists.add(s_snorm, j, 1);
       }
     }
@@ -1508,7 +1495,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     // grids whose V-cycles diverged continue as SOR from their current
     // potential with the boundary values set again (pb_solver.rs:1118-1125)
     bool switched = false;
-    std::vector<int> redo;
+    std::vector<int> redo, now_sor;
     for (int j = 0; j < nj; j++)
       if (hs[j].status == kDiverged) {
         phi_now[j] = hs[j].cur ? hd[j].phi2 : hd[j].phi;
@@ -1516,8 +1503,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           redo.push_back(j);
         else
           pb_boundary(c_, jobs[j].g, phi_now[j], *jobs[j].atoms, jobs[j].bc);
-        // SOR sweeps start from e = 0 (the V-cycles leave their last correction)
-        RSTG_CUDA(cudaMemsetAsync(hl[(size_t)j * kMaxLev].e, 0, padded_n(jobs[j].g) * 4, st));
+        now_sor.push_back(j);
         hs[j].status = kSor;
         hs[j].om = 1.0;
         hs[j].sor_it = 0;
@@ -1525,7 +1511,10 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
         switched = true;
       }
     dh_launch(redo);
-    if (switched) RSTG_CUDA(cudaMemcpyAsync(dS, hs.data(), sizeof(JobState) * nj, cudaMemcpyHostToDevice, st));
+    if (switched) {
+      RSTG_CUDA(cudaMemcpyAsync(dS, hs.data(), sizeof(JobState) * nj, cudaMemcpyHostToDevice, st));
+      sor_residuals(now_sor);  // of the current potential with its boundary values set again
+    }
     std::vector<int> k2;
     for (int j = 0; j < nj; j++)
       if (hs[j].status == kMg || hs[j].status == kSor) {
