@@ -972,6 +972,18 @@ __global__ void k_maxabs64(const JobD* __restrict__ J, double* __restrict__ M) {
 }
 
 long long cdiv(long long n, int t) { return (n + t - 1) / t; }
+// FP64 pool regions of a job, in units of g.n(): phi, phi2, rho (unless it
+// uses another job's), then for solvated jobs ex, ey, ez, kbar^2
+struct F64Lay {
+  size_t rho, maps, total;
+};
+F64Lay f64_lay(const PbJob& J) {
+  F64Lay f;
+  f.rho = 2;
+  f.maps = J.rho_of >= 0 ? 2 : 3;
+  f.total = f.maps + (J.uniform ? 0 : 4);
+  return f;
+}
 // FP32 and code arrays: rows padded to a multiple of 4 points (16 bytes of FP32)
 int pitch(const PbGeom& g) { return (int)((g.nx + 3) & ~3); }
 size_t padded_n(const PbGeom& g) { return (size_t)pitch(g) * g.ny * g.nz; }
@@ -1054,7 +1066,12 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     Lay& Y = lay[j];
     size_t n = J.g.n();
     Y.o64 = n64;
-    n64 += (J.uniform ? 3 : 7) * n;  // phi, rho, (4 maps), phi2
+    if (J.rho_of >= j || (J.rho_of >= 0 && (jobs[J.rho_of].atoms != J.atoms || jobs[J.rho_of].g.n() != J.g.n() ||
+                                             jobs[J.rho_of].g.ox != J.g.ox || jobs[J.rho_of].g.oy != J.g.oy ||
+                                             jobs[J.rho_of].g.oz != J.g.oz || jobs[J.rho_of].g.h != J.g.h ||
+                                             jobs[J.rho_of].g.nx != J.g.nx || jobs[J.rho_of].g.ny != J.g.ny)))
+      throw Error(RSTG_ERR_INVALID, "PB job shares the charge map of a job with another grid or atom set");
+    n64 += f64_lay(J).total * n;
     n64 = (n64 + 63) & ~(size_t)63;
     PbGeom g = J.g;
     Y.lv[0] = g;
@@ -1100,9 +1117,11 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     PbJob& J = jobs[j];
     size_t n = J.g.n();
     double* base = P64 + lay[j].o64;
-    double *phi = base, *rho = base + n;
-    double *ex = J.uniform ? nullptr : base + 2 * n, *ey = J.uniform ? nullptr : base + 3 * n,
-           *ez = J.uniform ? nullptr : base + 4 * n, *k2 = J.uniform ? nullptr : base + 5 * n;
+    const F64Lay f = f64_lay(J);
+    double *phi = base, *rho = J.rho_of >= 0 ? nullptr : base + f.rho * n;
+    double* m = base + f.maps * n;
+    double *ex = J.uniform ? nullptr : m, *ey = J.uniform ? nullptr : m + n, *ez = J.uniform ? nullptr : m + 2 * n,
+           *k2 = J.uniform ? nullptr : m + 3 * n;
     pb_maps_into(c_, J.g, *J.atoms, p, J.ein, J.eout, J.kap, J.ionic, rho, ex, ey, ez, k2);
     RSTG_CUDA(cudaMemsetAsync(phi, 0, n * 8, st));
     if (J.bc.kind != 1) pb_boundary(c_, J.g, phi, *J.atoms, J.bc);
@@ -1165,14 +1184,15 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     double* base = P64 + Y.o64;
     JobD& d = hd[j];
     std::memset(&d, 0, sizeof(d));
+    const F64Lay f = f64_lay(J);
     d.phi = base;
-    d.phi2 = base + (J.uniform ? 2 : 6) * n;
-    d.rho = base + n;
+    d.phi2 = base + n;
+    d.rho = J.rho_of >= 0 ? hd[J.rho_of].rho : base + f.rho * n;
     if (!J.uniform) {
-      d.ex = base + 2 * n;
-      d.ey = base + 3 * n;
-      d.ez = base + 4 * n;
-      d.k2 = base + 5 * n;
+      d.ex = base + f.maps * n;
+      d.ey = base + (f.maps + 1) * n;
+      d.ez = base + (f.maps + 2) * n;
+      d.k2 = base + (f.maps + 3) * n;
     }
     d.cd = P8 + Y.o8[0];
     d.px = pitch(J.g);
@@ -1650,6 +1670,7 @@ void pb_polar_batch(Ctx* c, cudaStream_t st, PbBatchEngine& eng, const rstg_pb_p
         PbJob J = make(i, s, coarse[i]);
         J.tol = p.tolerance * 10.0;
         J.energy = false;
+        if (s == 1) J.rho_of = (int)cj.size() - 1;  // same grid and atoms as the solvated solve
         cphi[2 * i + s] = DevBuf(coarse[i].n() * 8, st);
         outp.push_back(cphi[2 * i + s].as<double>());
         cj.push_back(J);
@@ -1666,6 +1687,7 @@ void pb_polar_batch(Ctx* c, cudaStream_t st, PbBatchEngine& eng, const rstg_pb_p
     if (!A[i]) continue;
     for (int s = 0; s < 2; s++) {
       PbJob J = make(i, s, fine[i]);
+      if (s == 1) J.rho_of = (int)fj.size() - 1;  // same grid and atoms as the solvated solve
       if (focus && ok[2 * i + s]) {
         J.bc.kind = 2;
         J.bc.cg = &coarse[i];

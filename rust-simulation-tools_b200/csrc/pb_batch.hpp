@@ -18,6 +18,7 @@ struct PbJob {
   double tol = 1e-6;
   int64_t maxit = 10000;
   bool energy = true;    // 0.5 sum q phi(atom) wanted
+  int rho_of = -1;       // index of an earlier job of the batch with the same grid and atoms: use its charge map
   // results
   PbSolveStats stats{};
   double e = 0.0;        // energy (kcal/mol) when requested
