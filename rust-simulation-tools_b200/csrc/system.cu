@@ -1418,10 +1418,12 @@ void System::run_pb(const void* frames, bool f64, bool host_in, int64_t F, rstg_
   const Topology* T[3] = {&split.complex, &split.rec, &split.lig};
   const std::vector<int64_t>* sel[3] = {nullptr, &split.rec_atoms, &split.lig_atoms};
   int64_t chunk = pb_frames_per_batch;
-  if (chunk <= 0) {  // device memory budget: at most 60 % of the free memory and 24 GB
+  if (chunk <= 0) {  // device memory budget: at most 60 % of the free memory and 64 GB
+    // (every lock-step cycle has a fixed cost, mostly the coarse levels, so
+    // fewer and larger batches are faster)
     size_t fr = 0, tot = 0;
     RSTG_CUDA(cudaMemGetInfo(&fr, &tot));
-    double budget = std::min(0.6 * (double)fr, 24e9);
+    double budget = std::min(0.6 * (double)fr, 64e9);
     chunk = std::max<int64_t>(1, (int64_t)(budget / (140.0 * (double)std::max<int64_t>(pb_points_estimate(), 1))));
   }
   std::vector<std::vector<double>> xs;
