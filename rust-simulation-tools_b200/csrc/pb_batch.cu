@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__
 // would store), rounded to FP32 as the next right-hand side, squares summed
 // per brick.  The correction is not cleared: the next cycle's first sweep
 // reads it as zero.
-__global__ void __launch_bounds__(256, 3) k_upres64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
+__global__ void __launch_bounds__(256, 4) k_upres64(WL w, const JobD* __restrict__ J, const LvlD* __restrict__ L,
                                                     const JobState* __restrict__ S, int want,
                                                     double* __restrict__ part, int nparts) {
   __shared__ double sh[32];
