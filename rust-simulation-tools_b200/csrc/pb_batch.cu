@@ -611,8 +611,7 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
     if (threadIdx.x == 0) part[(long long)j * nparts + lb] = t;
   }
 }
-#define k_sweep k_sweep_t<false>
-#define k_sor_sweep k_sweep_t<true>
+
 
 // SOR bookkeeping after a sweep and its update (pb_solver.rs:373-447): rms
 // of the sweep's updates from the sweep blocks' partial sums (fixed order),
@@ -1351,8 +1350,8 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   }
   const int K = std::max(1, chunk_cycles), KS = 4;  // cycles per chunk, SOR sweeps per cycle
   // the sweep's rings exceed the 48 KB default (set per call: the attribute is per device)
-  RSTG_CUDA(cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SwSmem)));
-  RSTG_CUDA(cudaFuncSetAttribute(k_sor_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SwSmem)));
+  RSTG_CUDA(cudaFuncSetAttribute(k_sweep_t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SwSmem)));
+  RSTG_CUDA(cudaFuncSetAttribute(k_sweep_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SwSmem)));
   bool use_graph = !profile && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
   std::vector<int> key;  // (job, status) pairs of the current lists
   std::vector<WL> wl;
@@ -1402,7 +1401,8 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       for (int s = 0; s < 3; s++) {
         const int flip = first ^ (s & 1), zero = (l == 0 && first == 0 && s == 0) ? 1 : 0;
         mark(l == 0 ? 0 : -1, dSweep, l, [&] {
-          k_sweep<<<go(ls[l].rb), kSwThreads, sizeof(SwSmem), st>>>(wl[ls[l].rb], dL, l, dS, flip, zero, nullptr, 0);
+          k_sweep_t<false><<<go(ls[l].rb), kSwThreads, sizeof(SwSmem), st>>>(wl[ls[l].rb], dL, l, dS, flip, zero,
+                                                                             nullptr, 0);
         });
         n++;
       }
@@ -1438,7 +1438,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           // sweep from e = 0 into e (the residual of the current potential is in rhs),
           // phi' = phi + e with the next residual, bookkeeping
           mark(-1, dSor, 0, [&] {
-            k_sor_sweep<<<go(s_sor), kSwThreads, sizeof(SwSmem), st>>>(wl[s_sor], dL, 0, dS, 1, 1, spart, nparts);
+            k_sweep_t<true><<<go(s_sor), kSwThreads, sizeof(SwSmem), st>>>(wl[s_sor], dL, 0, dS, 1, 1, spart, nparts);
             k_upres64<<<go(s_sres), kT, 0, st>>>(wl[s_sres], dJ, dL, dS, kSor, part, nparts);
             k_sor_norm<<<go(s_snorm), 256, 0, st>>>(wl[s_snorm], dJ, dS, spart, nparts);
           });
