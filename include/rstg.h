@@ -314,12 +314,15 @@ rstg_status rstg_system_last_stats(const rstg_system* s, int64_t* stats4);
  * set-up (maps, boundary values), the cycles and the finish (fallbacks,
  * energies).  Eight doubles; zeros for GB systems. */
 rstg_status rstg_system_pb_stats(const rstg_system* s, double* stats8);
-/* Frames per batched PB launch sequence (0: from the device memory budget). */
+/* Frames per batched PB launch sequence (0: from the device memory budget,
+ * at most 60 % of the free memory and 64 GB, about 140 bytes per grid point
+ * of the complex, receptor and ligand grids of a frame). */
 rstg_status rstg_system_set_pb_batch(rstg_system* s, int64_t frames);
 /* Profile mode of the batched PB engine (no reference counterpart): when on,
  * later runs launch the multigrid cycles without graph capture and time the
- * level-0 kernels with CUDA events.  rstg_system_pb_profile returns twelve
- * doubles, for the colour sweep, FP32 residual, FP64 residual and update:
+ * finest-level kernels with CUDA events.  rstg_system_pb_profile returns
+ * twelve doubles, for the full red-black sweep, FP32 residual, end-of-cycle
+ * update + FP64 residual and a fourth slot that is no longer used (zero):
  * total milliseconds [0..3], algorithmic DRAM bytes of the timed launches
  * [4..7] and launch counts [8..11], accumulated since profiling began. */
 rstg_status rstg_system_set_pb_profile(rstg_system* s, int32_t on);

@@ -781,11 +781,11 @@ class BindingSystem:
 
     def pb_profile(self) -> dict:
         """Per-kernel totals of the PB profile mode: ms, algorithmic DRAM bytes
-        and launches of the level-0 colour sweep, FP32 residual, FP64
-        residual and update."""
+        and launches of the finest-level full red-black sweep, FP32 residual
+        and end-of-cycle update + FP64 residual ("residual64")."""
         st = np.zeros(12)
         check(N.lib.rstg_system_pb_profile(self._h, _dp(st)))
-        names = ("sweep", "residual32", "residual64", "update64")
+        names = ("sweep", "residual32", "residual64")
         return {n: {"ms": st[k], "bytes": st[4 + k], "launches": int(st[8 + k])} for k, n in enumerate(names)}
 
     def set_pb_batch(self, frames: int) -> None:
