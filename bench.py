@@ -474,8 +474,16 @@ def main():
         top_k = int(np.argmax(kms[:n.value]))
         fl_k = max(int(np.argmax(np.where(kfl[:n.value] > 0, kms[:n.value], -1))), 0)
         ach = kfl[fl_k] / (kms[fl_k] / 1000.0) / 1e12
+        # DRAM traffic of one k_pairs launch: ncu dram read + write of a 64-frame
+        # launch of this workload (19.6 MB, profiles/mmgbsa_fused_w2_5050atoms_ncu.md),
+        # scaled by frames to this run's launches (the engine batches at most 256
+        # frames); the traffic is coordinates, radii and per-block sums, in
+        # proportion to frames
+        per_launch = F / -(-F // 256)
+        traffic = 19.6e6 / 64 * per_launch if kn[fl_k] == "pairs" else None
         extras["roofline"] = {"bound": "fp32", "kernel": kn[fl_k], "achieved": ach, "peak": float(cal[0]),
-                              "unit": "TFLOP/s", "frac": ach / cal[0], "traffic": None,
+                              "unit": "TFLOP/s", "frac": ach / cal[0], "traffic": traffic,
+                              "traffic_source": "ncu capture of a 64-frame launch scaled by frames per launch",
                               "peak_source": "measured FP32 FMA loop (rstg_calibrate) on this GPU",
                               "dominant_kernel": kn[top_k], "kernel_share": share,
                               "kernel_ms_per_1000_frames": {kn[k]: round(float(kms[k]) * 1000.0 / F, 3)
