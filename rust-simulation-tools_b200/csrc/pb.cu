@@ -784,7 +784,8 @@ static void charge_into(Ctx* c, const PbGeom& g, const AtomsDev& A, double* rho)
   k_scatter<<<nblk((long long)idx.size(), 256), 256, 0, st>>>(di.as<long long>(), dv.as<double>(), (int)idx.size(),
                                                               rho);
   launched(c);
-  RSTG_CUDA(cudaStreamSynchronize(st));  // the host vectors above go out of scope
+  // no synchronisation: copies from pageable host memory are staged before
+  // cudaMemcpyAsync returns, and the device buffers are freed in stream order
 }
 
 static void charge_map(Ctx* c, const PbGeom& g, const AtomsDev& A, DevBuf& rho) {
@@ -849,7 +850,6 @@ static void dielectric_into(Ctx* c, const PbGeom& g, const AtomsDev& A, double p
     RSTG_CUDA(cudaMemcpyAsync(doff.p, offs.data(), offs.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
     k_ses<<<nblk(n, 256), 256, 0, st>>>(gd, ext.as<uint8_t>(), doff.as<int4>(), (int)offs.size(), inside.as<uint8_t>());
     launched(c);
-    RSTG_CUDA(cudaStreamSynchronize(st));
   }
   HashBuf he(pb_build_hash(A.hx, A.max_r + g.h), st);
   DevBuf ovf(8, st);
@@ -884,7 +884,6 @@ static void kappa_into(Ctx* c, const PbGeom& g, const AtomsDev& A, double ion, d
   HashBuf hk(pb_build_hash(A.hx, A.max_r + ion), st);
   k_kappa<<<nblk(n, 256), 256, 0, st>>>(gdev(g), hk.d, A.xyz.as<double>(), A.r.as<double>(), ion, kbs, k2);
   launched(c);
-  RSTG_CUDA(cudaStreamSynchronize(st));
 }
 
 static void kappa_map(Ctx* c, Maps& M, const AtomsDev& A, double ion, double kap, double eps_s, bool ionic) {
