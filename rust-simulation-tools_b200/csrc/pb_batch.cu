@@ -376,11 +376,11 @@ constexpr int kSwEY = kSwTY + 4;  // correction rows: y in [yt-2, yt+TY+2)
 constexpr int kSwRY = kSwTY + 2;  // right-hand-side rows: y in [yt-1, yt+TY+1)
 constexpr int kSwCY = kSwTY + 3;  // code rows: y in [yt-2, yt+TY+1)
 constexpr int kSwNE = 8, kSwNR = 8, kSwNC = 8;  // ring depths in planes (slot = plane & (depth - 1))
-// round 0: even points of plane s+2 inside the tile's x range, 16 per row, rows yt-1 .. yt+TY;
-// round 1: odd points of plane s (threads < TY*16), then the even points of plane s+2 on the
+// first point of a thread: even points of plane s+2 inside the tile's x range, 16 per row, rows yt-1 .. yt+TY;
+// second point: odd points of plane s (threads < TY*16), then the even points of plane s+2 on the
 // x halo (one per row: x = xt-1 or xt+TX)
 static_assert(kSwTX == 32 && (kSwTY + 2) * 16 == kSwThreads && kSwTY * 16 + kSwTY + 2 <= kSwThreads,
-              "point rounds of the sweep");
+              "point assignment of the sweep");
 static_assert(kSwEY * (kSwW / 4) <= kSwThreads && kSwRY * (kSwW / 4) <= kSwThreads &&
                   kSwCY * (kSwW / 4) <= kSwThreads && kSwTY * (kSwTX / 4) <= kSwThreads,
               "one copy chunk and one store per thread and plane");
@@ -504,8 +504,8 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
   auto load_c = [&](int p) {
     if (cso >= 0 && p >= 0 && p < d.nz) cp_async4(&sm.c[sc_(p)][cso], d.cd + cgo + (long long)d.sz * p);
   };
-  // this thread's points.  Main (round 0): even point of row ym = yt-1+tid/16
-  // at x = xt + 2(tid%16) + ((xt + ym + p) & 1).  Round 1: odd point of row
+  // this thread's points.  Main (first point): even point of row ym = yt-1+tid/16
+  // at x = xt + 2(tid%16) + ((xt + ym + p) & 1).  Second point: odd point of row
   // yo = yt + tid/16 at x = xt + 2(tid%16) + ((xt + yo + p + 1) & 1), or for
   // threads TY*16 .. TY*16+TY+1 the halo even point of row yh = yt-1+(tid-TY*16)
   // at xt-1 or xt+TX, whichever has the even colour.
@@ -552,8 +552,8 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
     const float dv = sw_update<kSorMode>(d, om, P.E0, P.Em, P.Ep, P.R, P.C0, P.Cm, off, g + P.gp);
     if (kSorMode && own) acc += (double)dv * (double)dv;
   };
-  const bool m_own = ym >= yt && ym < yt + kSwTY;  // main-round row inside the tile (not the y halo)
-  // even points of plane p: main round and halo
+  const bool m_own = ym >= yt && ym < yt + kSwTY;  // first-point row inside the tile (not the y halo)
+  // even points of plane p: first point and x-halo point
   auto even = [&](int p) {
     if (p < 1 || p > d.nz - 2) return;
     const Planes P = planes(p);

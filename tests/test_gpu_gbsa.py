@@ -1,6 +1,6 @@
 """GPU parity of the MM-GBSA path against the CPU restatement.
 
-Tolerances (stated per the north star):
+Tolerances:
   * plain FP64 form vs the reference-faithful restatement: relative 1e-10 on
     every energy, 1e-12 on Born radii, per-atom SASA bit-identical;
   * fused mixed-precision form vs the accurate restatement: per-frame

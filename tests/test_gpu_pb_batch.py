@@ -1,7 +1,7 @@
 """GPU parity of the batched mixed-precision PB engine (fused BindingSystem
 with PbParams).
 
-Tolerances (stated per the north star):
+Tolerances:
   * per-frame binding terms within 1e-3 kcal/mol of the CPU restatement
     (accurate receptor x ligand MM differences), subsystem PB energies within
     1e-6 relative;
