@@ -339,8 +339,8 @@ def large_mixed(rst, ctx, gb_requests=6, gb_frames=24, pb_requests=2, pb_frames=
             "gb_frames_per_request": gb_frames, "pb_requests": pb_requests, "pb_frames_per_request": pb_frames,
             "frames": frames, "frames_per_s": frames / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "pb_stats": psys.pb_stats(), "abs_diff_vs_plain_fp64_frame1_kcal": err,
-            "note": "delta_mm of the plain form carries the reference's cancellation (see DESIGN); polar and SA "
-                    "terms compared"}
+            "note": "delta_mm of the plain form carries the reference's FP64 cancellation error (it subtracts "
+                    "sums of ~1e5 kcal/mol); polar and SA terms compared"}
 
 
 def main():
@@ -475,7 +475,7 @@ def main():
         fl_k = max(int(np.argmax(np.where(kfl[:n.value] > 0, kms[:n.value], -1))), 0)
         ach = kfl[fl_k] / (kms[fl_k] / 1000.0) / 1e12
         # DRAM traffic of one k_pairs launch: ncu dram read + write of a 64-frame
-        # launch of this workload (19.6 MB, profiles/mmgbsa_fused_w2_5050atoms_ncu.md),
+        # launch of this workload (19.6 MB, the committed ncu summary of k_pairs),
         # scaled by frames to this run's launches (the engine batches at most 256
         # frames); the traffic is coordinates, radii and per-block sums, in
         # proportion to frames

@@ -40,7 +40,10 @@
 
 namespace rstg {
 
-static constexpr float kSasaBand = 2e-4f;  // A^2, FP32 error bound x 10
+// A^2: ten times the FP32 error bound of a point-to-neighbour squared distance
+// at these coordinates; SASA point tests closer than this to the threshold are
+// redone in FP64 with the reference's rounding
+static constexpr float kSasaBand = 2e-4f;
 static constexpr float kNbGuard2 = 3.5f * 3.5f;
 static constexpr int kSasaWarps = 4;
 
