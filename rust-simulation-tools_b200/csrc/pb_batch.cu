@@ -1035,6 +1035,12 @@ struct Lists {
 
 }  // namespace
 
+void PbBatchEngine::release() {
+  if (graph_) cudaGraphExecDestroy(graph_);
+  graph_ = nullptr;
+  for (DevBuf* b : {&pool64_, &pool32_, &pool8_, &desc_, &part_, &small_, &lists_}) *b = DevBuf();
+}
+
 PbBatchEngine::~PbBatchEngine() {
   if (graph_) cudaGraphExecDestroy(graph_);
   for (cudaEvent_t e : prof_events_) cudaEventDestroy(e);

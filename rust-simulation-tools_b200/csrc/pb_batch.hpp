@@ -58,6 +58,8 @@ class PbBatchEngine {
   // phi_out[j] (device arrays of g.n() doubles, may be null per job).
   void solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, const std::vector<double*>* phi_out = nullptr);
   void set_stream(cudaStream_t s) { st_ = s; }
+  // Frees the device pools (kept between solves otherwise); statistics stay.
+  void release();
   PbBatchStats stats;
   PbProfile prof;
   bool profile = false;  // time the level-0 kernels with events (no graph capture)

@@ -1302,6 +1302,7 @@ void System::release_buffers() {
                     &res_buf, &dec_buf, &diag})
     *b = DevBuf();
   buf_frames = 0;
+  if (pbe) pbe->release();  // the PB pools are part of the footprint a server accounts for
 }
 
 void System::profile(const float* d_frames, int64_t F, int32_t* n, char* names, double* ms, double* flops,

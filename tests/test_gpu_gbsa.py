@@ -313,6 +313,35 @@ def test_server_results_same_alone_and_in_mix(rst, sysdata):
     srv.close()
 
 
+def test_server_evicts_idle_systems_under_budget(rst, sysdata):
+    # a budget smaller than any request: requests run one at a time and each
+    # admission evicts the idle system's resident buffers (and its captured
+    # graph); re-admitted systems rebuild them and give the same bits
+    from rust_simulation_tools import synthetic as S
+    import tempfile, os
+
+    s, fr, prm, _ = sysdata
+    top = rst.read_prmtop(prm)
+    s2 = S.make_system(150, 20, seed=33)
+    fr2 = S.make_frames(s2, 4, seed=34)
+    d = tempfile.mkdtemp()
+    S.write_prmtop(s2, os.path.join(d, "c.prmtop"))
+    top2 = rst.read_prmtop(os.path.join(d, "c.prmtop"))
+    A = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues)
+    B = rst.BindingSystem(top2, s2.receptor_residues, s2.ligand_residues)
+    alone_a, alone_b = A.run(fr), B.run(fr2)
+    srv = rst.Server(memory_budget_bytes=1, max_inflight=2)
+    ids = [srv.submit(A, fr), srv.submit(B, fr2), srv.submit(A, fr), srv.submit(B, fr2[1:])]
+    res = [srv.wait(i, 60000) for i in ids]
+    st = srv.stats()
+    srv.close()
+    np.testing.assert_array_equal(res[0], alone_a)
+    np.testing.assert_array_equal(res[1], alone_b)
+    np.testing.assert_array_equal(res[2], alone_a)
+    np.testing.assert_array_equal(res[3], alone_b[1:])
+    assert st["completed"] == 4
+
+
 def test_gb_cache_reuses_radii(rst, oracle, sysdata):
     # gb_energy.rs:66-120,372-387: first call computes and caches the radii;
     # a frame within the RMSD threshold reuses them (energy from the cached

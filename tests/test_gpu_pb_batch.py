@@ -127,6 +127,26 @@ def test_server_mixes_pb_and_gb_requests(rst, small):
     assert st["completed"] == 4
 
 
+def test_server_evicts_pb_systems_under_budget(rst, small):
+    # a budget smaller than any request: one request at a time, each admission
+    # releases the idle system's resident batch buffers (PB pools included);
+    # results keep their bits when the systems come back
+    s, fr, prm = small
+    top = rst.read_prmtop(prm)
+    pbs = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues,
+                            pb_params=rst.PbParams(grid_spacing=0.6, grid_buffer=4.0))
+    gbs = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues)
+    alone_p, alone_g = pbs.run(fr), gbs.run(fr)
+    srv = rst.Server(memory_budget_bytes=1, max_inflight=2)
+    ids = [srv.submit(pbs, fr), srv.submit(gbs, fr), srv.submit(pbs, fr[:2]), srv.submit(gbs, fr)]
+    res = [srv.wait(i, 600000) for i in ids]
+    srv.close()
+    np.testing.assert_array_equal(res[0], alone_p)
+    np.testing.assert_array_equal(res[1], alone_g)
+    np.testing.assert_array_equal(res[2], alone_p[:2])
+    np.testing.assert_array_equal(res[3], alone_g)
+
+
 def test_system_outlives_server_after_growing_buffers(rst, small):
     # buffers a system allocates while a server runs its request belong to a
     # server slot stream; destroying the system after the server must be safe
