@@ -370,7 +370,7 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
 // z planes per block: long marches on the finest level, short ones on the
 // coarse levels (few tiles per grid there, so more chunks keep the SMs busy)
 constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 288, kSwZC0 = 48, kSwZC1 = 16;
-int sweep_chunk(int lvl) { return lvl == 0 ? kSwZC0 : kSwZC1; }
+int sweep_chunk(int lvl) { return lvl == 0 ? kSwZC0 : (lvl == 1 ? kSwZC1 : 8); }
 constexpr int kSwW = kSwTX + 8;   // shared row: x in [xt-4, xt+TX+4), 16-byte chunks
 constexpr int kSwEY = kSwTY + 4;  // correction rows: y in [yt-2, yt+TY+2)
 constexpr int kSwRY = kSwTY + 2;  // right-hand-side rows: y in [yt-1, yt+TY+1)
