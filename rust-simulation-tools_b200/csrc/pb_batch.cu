@@ -389,6 +389,9 @@ struct SwSmem {
   float e[kSwNE][kSwEY * kSwW];
   float r[kSwNR][kSwRY * kSwW];
   uint8_t c[kSwNC][kSwCY * kSwW];
+  // faces of every eps_in / eps_out pattern (bit k set: face k is eps_in;
+  // faces x+, x-, y+, y-, z+, z-): [0] x+, x-, y+, y-; [1] z+, z-, their sum
+  float4 tf[2][64];
 };
 
 __device__ __forceinline__ void cp_async16(void* s, const void* g) {
@@ -411,10 +414,11 @@ __device__ __forceinline__ void cp_async_wait() {
 // Multigrid smoothing divides with the fast reciprocal; the SOR fallback
 // (pb_solver.rs:373-447) with the exact division, as a plain sweep does.
 template <bool kExact>
-__device__ __forceinline__ float sw_update(const Lv& d, float om, float* __restrict__ E0,
-                                           const float* __restrict__ Em, const float* __restrict__ Ep,
-                                           const float* __restrict__ R, const uint8_t* __restrict__ C0,
-                                           const uint8_t* __restrict__ Cm, int off, int gi) {
+__device__ __forceinline__ float sw_update(const Lv& d, const float4 (*__restrict__ tf)[64], float om,
+                                           float* __restrict__ E0, const float* __restrict__ Em,
+                                           const float* __restrict__ Ep, const float* __restrict__ R,
+                                           const uint8_t* __restrict__ C0, const uint8_t* __restrict__ Cm, int off,
+                                           int gi) {
   float* ec = E0 + off;
   const float xm = ec[-1], xp = ec[1], ym = ec[-kSwW], yp = ec[kSwW], zm = Em[off], zp = Ep[off], old = ec[0];
   const float rhs = R[off - kSwW];
@@ -424,24 +428,21 @@ __device__ __forceinline__ float sw_update(const Lv& d, float om, float* __restr
     dg = 6.0f * d.w6;
   } else {
     const unsigned c0 = C0[off], cxm = C0[off - 1], cym = C0[off - kSwW], czm = Cm[off];
-    float a, b, c, dd, f, g;
+    const float k2 = (c0 & 64u) ? d.kb : 0.0f;
     if (((c0 & 0x2Au) | (cxm & 0x2u) | (cym & 0x8u) | (czm & 0x20u)) == 0u) {  // no face crosses the surface
-      a = (c0 & 0x1u) ? d.fin : d.fout;
-      b = (cxm & 0x1u) ? d.fin : d.fout;
-      c = (c0 & 0x4u) ? d.fin : d.fout;
-      dd = (cym & 0x4u) ? d.fin : d.fout;
-      f = (c0 & 0x10u) ? d.fin : d.fout;
-      g = (czm & 0x10u) ? d.fin : d.fout;
+      const unsigned pat = (c0 & 0x15u) | ((cxm & 0x1u) << 1) | ((cym & 0x4u) << 1) | ((czm & 0x10u) << 1);
+      const float4 u = tf[0][pat], v = tf[1][pat];
+      ns = ((u.x * xp + u.y * xm) + (u.z * yp + u.w * ym) + (v.x * zp + v.y * zm)) * d.ih;
+      dg = fmaf(v.z, d.ih, k2);
     } else {
-      a = face(c0 & 3u, d.ex, gi, d.fin, d.fout);
-      b = face(cxm & 3u, d.ex, gi - 1, d.fin, d.fout);
-      c = face((c0 >> 2) & 3u, d.ey, gi, d.fin, d.fout);
-      dd = face((cym >> 2) & 3u, d.ey, gi - d.sy, d.fin, d.fout);
-      f = face((c0 >> 4) & 3u, d.ez, gi, d.fin, d.fout);
-      g = face((czm >> 4) & 3u, d.ez, gi - d.sz, d.fin, d.fout);
+      const float a = face(c0 & 3u, d.ex, gi, d.fin, d.fout), b = face(cxm & 3u, d.ex, gi - 1, d.fin, d.fout),
+                  c = face((c0 >> 2) & 3u, d.ey, gi, d.fin, d.fout),
+                  dd = face((cym >> 2) & 3u, d.ey, gi - d.sy, d.fin, d.fout),
+                  f = face((c0 >> 4) & 3u, d.ez, gi, d.fin, d.fout),
+                  g = face((czm >> 4) & 3u, d.ez, gi - d.sz, d.fin, d.fout);
+      ns = ((a * xp + b * xm) + (c * yp + dd * ym) + (f * zp + g * zm)) * d.ih;
+      dg = fmaf((a + b) + (c + dd) + (f + g), d.ih, k2);
     }
-    ns = ((a * xp + b * xm) + (c * yp + dd * ym) + (f * zp + g * zm)) * d.ih;
-    dg = ((a + b) + (c + dd) + (f + g)) * d.ih + ((c0 & 64u) ? d.kb : 0.0f);
   }
   const float gs = kExact ? (ns + rhs) / dg : __fdividef(ns + rhs, dg);
   const float dv = gs - old;
@@ -549,7 +550,7 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
   };
   auto update = [&](const Planes& P, int x, int off, int g, bool own) {
     if (x < 1 || x > d.nx - 2) return;
-    const float dv = sw_update<kSorMode>(d, om, P.E0, P.Em, P.Ep, P.R, P.C0, P.Cm, off, g + P.gp);
+    const float dv = sw_update<kSorMode>(d, sm.tf, om, P.E0, P.Em, P.Ep, P.R, P.C0, P.Cm, off, g + P.gp);
     if (kSorMode && own) acc += (double)dv * (double)dv;
   };
   const bool m_own = ym >= yt && ym < yt + kSwTY;  // first-point row inside the tile (not the y halo)
@@ -581,6 +582,12 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
   for (int p = z0 - 1; p <= z0 + 2; p++) load_r(p);
   for (int p = z0 - 2; p <= z0 + 2; p++) load_c(p);
   cp_async_commit();
+  if (!d.uni && tid < 64) {  // face table (read after the barrier below)
+    const float a = (tid & 1) ? d.fin : d.fout, b = (tid & 2) ? d.fin : d.fout, c = (tid & 4) ? d.fin : d.fout,
+                dd = (tid & 8) ? d.fin : d.fout, f = (tid & 16) ? d.fin : d.fout, g = (tid & 32) ? d.fin : d.fout;
+    sm.tf[0][tid] = make_float4(a, b, c, dd);
+    sm.tf[1][tid] = make_float4(f, g, (a + b) + (c + dd) + (f + g), 0.0f);
+  }
   load_e(z0 + 4);
   load_r(z0 + 3);
   load_c(z0 + 3);
