@@ -56,9 +56,39 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def workload(n_frames, rank):
-    from rust_simulation_tools import synthetic as S
+def _synthetic():
+    """The seeded input generator, loaded from its file without importing the
+    package (whose __init__ maps librstg.so): the reference arm must run on
+    the host cores with no GPU library in the process."""
+    name = "_rstg_synthetic"
+    if name not in sys.modules:
+        import importlib.util
 
+        spec = importlib.util.spec_from_file_location(
+            name, os.path.join(ROOT, "rust-simulation-tools_b200", "rust_simulation_tools", "synthetic.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+def host_facts():
+    """CPU model and logical core count of this host (reported beside every
+    CPU number)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
+
+
+def workload(n_frames, rank):
+    S = _synthetic()
     s = S.make_system(5000, 50, seed=1002)
     fr = S.make_frames(s, n_frames, seed=2002 + 7919 * rank)
     return s, fr
@@ -105,12 +135,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def cpu_baseline(s, fr, n_sample):
+def cpu_baseline(s, fr, n_sample, gpu_rows=None, gpu_dec=None, n_check=2):
+    """The CPU restatement of the reference (faithful mode, all host threads)
+    timed on the first n_sample frames.  With the GPU's rows and per-residue
+    terms for those frames, the largest differences against the accurate
+    restatement (binding terms, per-residue terms) and against the faithful
+    one (polar and SA binding terms) on the first n_check frames ride along,
+    untimed, so the line carries its own parity."""
     import oracle as O
 
     O.build()
     d = tempfile.mkdtemp()
-    from rust_simulation_tools import synthetic as S
+    S = _synthetic()
 
     S.write_prmtop(s, os.path.join(d, "w.prmtop"))
     top = O.Topology.load(os.path.join(d, "w.prmtop"))
@@ -118,13 +154,33 @@ def cpu_baseline(s, fr, n_sample):
     gb = O.gb_params("obc2", solvent_dielectric=78.5)
     sa = O.sa_params(n_points=NPTS)
     t = time.perf_counter()
-    O.binding_frames(top, x, s.receptor_residues, s.ligand_residues, gb=gb, sa=sa)
+    faithful = O.binding_frames(top, x, s.receptor_residues, s.ligand_residues, gb=gb, sa=sa)
     for f in range(n_sample):  # decomposition of every frame, as the GPU step does
         O.decompose(top, x[f], s.receptor_residues, s.ligand_residues, gb, sa)
     dt = time.perf_counter() - t
-    return {"value": n_sample / dt, "unit": "frames/s", "cores": O.threads(), "kind": "port",
-            "sample": f"{n_sample} frames of the 5,050-atom workload, binding frame + decomposition, "
-                      f"C++ restatement of the reference, {O.threads()} OpenMP threads"}
+    hf = host_facts()
+    out = {"value": n_sample / dt, "unit": "frames/s", "cores": O.threads(), "kind": "port",
+           "threads": O.threads(), "nproc": hf["nproc"], "cpu_model": hf["cpu_model"],
+           "sample": f"{n_sample} frames of the 5,050-atom workload, binding frame + decomposition, "
+                     f"C++ restatement of the reference, {O.threads()} OpenMP threads on a "
+                     f"{hf['nproc']}-thread host"}
+    if gpu_rows is not None:
+        nc = min(n_check, n_sample)
+        keys = ("delta_mm", "delta_polar", "delta_sa", "delta_total")
+        acc = O.binding_frames(top, x[:nc], s.receptor_residues, s.ligand_residues, gb=gb, sa=sa, accurate=True)
+        par = {"frames": nc, "tolerance_kcal": {"frame": 1e-3, "residue": 1e-4},
+               "max_abs_vs_accurate_oracle": {k: float(np.abs(gpu_rows[:nc, 9 + i] - acc[:, 9 + i]).max())
+                                              for i, k in enumerate(keys)},
+               "max_abs_vs_faithful_oracle": {k: float(np.abs(gpu_rows[:nc, 9 + i] - faithful[:nc, 9 + i]).max())
+                                              for i, k in enumerate(keys) if k in ("delta_polar", "delta_sa")}}
+        if gpu_dec is not None:
+            worst = 0.0
+            for f in range(nc):
+                ro, lo = O.decompose(top, x[f], s.receptor_residues, s.ligand_residues, gb, sa, accurate=True)
+                worst = max(worst, float(np.abs(gpu_dec[f] - np.concatenate([ro, lo])).max()))
+            par["max_abs_residue_vs_accurate_oracle"] = worst
+        out["parity"] = par
+    return out
 
 
 PB = dict(grid_spacing=0.5, grid_buffer=12.0, fillratio=0.0)  # linearised PB, DH boundary, no focusing
@@ -144,7 +200,7 @@ def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs):
     (per-frame solve cost varies: some frames stop at the cycle cap, some
     diverge and finish with SOR)."""
     import torch
-    from rust_simulation_tools import synthetic as S
+    S = _synthetic()
 
     s, fr = S.workload(3, n_frames=n_frames)
     d = tempfile.mkdtemp()
@@ -205,6 +261,7 @@ def run_reference(args):
             "config": {"workload": "MM-GBSA + per-residue decomposition, 5,000 + 50 atoms, 1,000 frames",
                        "sample_frames_per_step": args.ref_frames},
             "cpu_baseline": {"value": v, "unit": "frames/s", "cores": r["cores"], "kind": "port",
+                             "threads": r["threads"], "nproc": r["nproc"], "cpu_model": r["cpu_model"],
                              "sample": r["sample"]},
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -225,7 +282,7 @@ def serving_stream(rst, ctx, n_req, seed=4):
     one-at-a-time capacity; beside it the same requests one at a time (fused
     engine, and plain FP64 form from its per-frame time on each system) on the
     same arrival times."""
-    from rust_simulation_tools import synthetic as S
+    S = _synthetic()
 
     rng = np.random.default_rng(seed)
     d = tempfile.mkdtemp()
@@ -301,7 +358,7 @@ def large_mixed(rst, ctx, gb_requests=6, gb_frames=24, pb_requests=2, pb_frames=
     """Bounded large mixed load: 25,000 + 80 atoms, MM-GBSA (SASA 960 points)
     and MM-PBSA (0.5 A grids of ~193^3, DH boundary) requests interleaved in
     one serving loop; errors against the plain FP64 form on one frame."""
-    from rust_simulation_tools import synthetic as S
+    S = _synthetic()
 
     s, fr = S.workload(5, n_frames=max(gb_frames, pb_frames) + 1)
     d = tempfile.mkdtemp()
@@ -393,7 +450,7 @@ def main():
     ctx = N.make_ctx(local, stream.cuda_stream)
     s, fr = workload(args.frames, rank)
     d = tempfile.mkdtemp()
-    from rust_simulation_tools import synthetic as S
+    S = _synthetic()
 
     S.write_prmtop(s, os.path.join(d, "w.prmtop"))
     top = rst.read_prmtop(os.path.join(d, "w.prmtop"))
@@ -502,7 +559,7 @@ def main():
                                    "form": "FP64, one subsystem per launch sequence, per frame, decomposition"}
             extras["speedup_vs_plain_gpu"] = value / world / pv
         if rank == 0 and world == 1 and args.ref_frames > 0:
-            extras["cpu_baseline"] = cpu_baseline(s, fr, args.ref_frames)
+            extras["cpu_baseline"] = cpu_baseline(s, fr, args.ref_frames, out_np, d_dec.cpu().numpy())
         if rank == 0 and world == 1 and args.serve_requests > 0:
             extras["serving"] = serving_stream(rst, ctx, args.serve_requests)
         if rank == 0 and world == 1 and args.pb_frames > 0:

@@ -12,7 +12,9 @@
 // this library holds it until the process exits.  Host code cannot use the
 // array's name as a device address, so the first call on each device resolves
 // the address with cudaGetSymbolAddress (with that device current) and caches
-// it; that first call should therefore come before any stream capture.  All
+// it with the id of the device's context (a device reset gives a new context,
+// and the address is then resolved again); that first call on a device, or
+// after a reset, should therefore come before any stream capture.  All
 // calls on a device share the array: calls whose kernels overlap on the GPU
 // (for example on two streams) race and must be serialised by the caller.
 // Every scratch element a call reads is written earlier in the same call, so
@@ -31,17 +33,52 @@ static __device__ __align__(256) double g_gb_scratch[kGbScratchDoubles];
 
 static std::mutex g_scratch_mu;
 static double* g_scratch_addr[kMaxDevices] = {};
+static unsigned long long g_scratch_ctx[kMaxDevices] = {};
 
-// Device address of g_gb_scratch on the current device (set up once per device).
+// Process-unique id of the calling thread's current CUDA context (0 when it
+// cannot be read).  After cudaDeviceReset the device gets a new primary
+// context, the module is loaded again and the array may sit at a new
+// address; the id tells the cached address apart from a stale one.  The
+// driver functions come through the runtime's entry-point query, so the
+// library needs no link against libcuda.
+static unsigned long long current_ctx_id() {
+  typedef int (*GetCurrent)(void**);
+  typedef int (*GetId)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (GetCurrent)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (GetId)f;
+    looked_up = true;
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, &id) == 0) return id;
+  return 0;
+}
+
+// Device address of g_gb_scratch on the current device.  Resolved once per
+// device and context (the caller has made the device current), and again
+// only when the device's context has changed.
 static double* scratch_on(int device) {
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_addr[device]) {
+  unsigned long long id = current_ctx_id();
+  if (!g_scratch_addr[device] || g_scratch_ctx[device] != id) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_gb_scratch);
     if (e != cudaSuccess || !p)
       throw Error(RSTG_ERR_CUDA, std::string("cudaGetSymbolAddress of the GB scratch array failed: ") +
                                      cudaGetErrorString(e));
     g_scratch_addr[device] = (double*)p;
+    g_scratch_ctx[device] = id;
   }
   return g_scratch_addr[device];
 }

@@ -116,19 +116,21 @@ struct Server {
   }
 
   // Releases idle systems' buffers (least recently used first) until `need`
-  // more bytes fit the budget; systems whose lock is taken are skipped.
+  // more bytes fit the budget.  A system whose lock is taken elsewhere, or a
+  // plain-mode system (its evaluator's buffers are not released here), keeps
+  // its bytes in the count and is passed over for the next candidate.
   void evict_for(int64_t need, System* keep) {
-    while (resident_total + need > opts.memory_budget_bytes) {
-      System* victim = nullptr;
-      int64_t oldest = INT64_MAX;
-      for (auto& kv : resident)
-        if (kv.first != keep && !busy.count(kv.first) && last_use[kv.first] < oldest) {
-          oldest = last_use[kv.first];
-          victim = kv.first;
-        }
-      if (!victim) return;
+    std::vector<std::pair<int64_t, System*>> order;
+    for (auto& kv : resident)
+      if (kv.first != keep && !busy.count(kv.first)) order.push_back({last_use[kv.first], kv.first});
+    std::sort(order.begin(), order.end());
+    for (auto& o : order) {
+      if (resident_total + need <= opts.memory_budget_bytes) return;
+      System* victim = o.second;
+      if (victim->opts.mode != RSTG_MODE_FUSED) continue;
       std::unique_lock<std::recursive_mutex> vl(victim->mu, std::try_to_lock);
-      if (vl.owns_lock() && victim->opts.mode == RSTG_MODE_FUSED) victim->release_buffers();
+      if (!vl.owns_lock()) continue;
+      victim->release_buffers();
       resident_total -= resident[victim];
       resident.erase(victim);
     }

@@ -2,13 +2,25 @@
 
 Every (frame, subsystem) evaluation is independent, so the frames are split
 into contiguous ranges, one per rank (one process per GPU), each rank runs
-its range through its own BindingSystem, and the per-frame rows are gathered
-back in frame order.  The statistics of binding.rs:704-743 are then taken
-over the gathered rows in that order, so they do not depend on the number of
-ranks.  torch.distributed is the plumbing (NCCL between GPUs, gloo on CPU);
-the gather moves 13 doubles per frame.
+its range through its own BindingSystem, and the per-frame rows are merged
+back in frame order on the host.  The statistics of binding.rs:704-743 are
+then taken over the merged rows in that order, so they do not depend on the
+number of ranks.
+
+The module carries no transport of its own: the caller hands in an
+``allgather(obj) -> list`` callable that returns every rank's object in rank
+order (13 doubles per frame cross it).  With torch.distributed that is::
+
+    def allgather(obj):
+        out = [None] * dist.get_world_size()
+        dist.all_gather_object(out, obj)
+        return out
+
+with mpi4py ``comm.allgather``; in one process ``lambda obj: [obj]``.
 """
 from __future__ import annotations
+
+from typing import Callable, Sequence
 
 import numpy as np
 
@@ -23,38 +35,46 @@ def frame_range(n_frames: int, rank: int, world: int) -> tuple[int, int]:
     return start, start + base + (1 if rank < extra else 0)
 
 
-def gather_rows(local: np.ndarray, n_frames: int, group=None) -> np.ndarray:
-    """All-gather the (rows, k) float64 blocks of every rank into (n_frames, k)
-    in rank (= frame) order."""
-    import torch
-    import torch.distributed as dist
+def merge_rows(blocks: Sequence[np.ndarray], n_frames: int) -> np.ndarray:
+    """The (n_frames, k) rows of all ranks in frame order, from the per-rank
+    (rows, k) blocks listed in rank order; each block must hold exactly its
+    rank's frame range."""
+    world = len(blocks)
+    if world < 1:
+        raise ValueError("no rank blocks to merge")
+    out = []
+    for r, b in enumerate(blocks):
+        a, e = frame_range(n_frames, r, world)
+        b = np.asarray(b, dtype=np.float64)
+        if b.ndim != 2 or b.shape[0] != e - a:
+            raise ValueError(f"rank {r} sent a block of shape {b.shape} for frames [{a}, {e})")
+        out.append(b)
+    return np.concatenate(out, axis=0)
 
-    world = dist.get_world_size(group)
+
+def gather_rows(local: np.ndarray, n_frames: int, rank: int, world: int,
+                allgather: Callable[[object], list]) -> np.ndarray:
+    """Every rank's (rows, k) float64 block, exchanged through ``allgather``
+    and merged into (n_frames, k) in frame order."""
+    a, b = frame_range(n_frames, rank, world)
     local = np.ascontiguousarray(local, dtype=np.float64)
-    k = local.shape[1]
-    counts = [frame_range(n_frames, r, world)[1] - frame_range(n_frames, r, world)[0] for r in range(world)]
-    if local.shape[0] != counts[dist.get_rank(group)]:
+    if local.shape[0] != b - a:
         raise ValueError("local rows do not match this rank's frame range")
-    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
-    m = max(counts)
-    buf = torch.zeros((m, k), dtype=torch.float64, device=dev)
-    if local.shape[0]:
-        buf[: local.shape[0]] = torch.from_numpy(local).to(dev)
-    parts = [torch.empty_like(buf) for _ in range(world)]
-    dist.all_gather(parts, buf, group=group)
-    return np.concatenate([parts[r][: counts[r]].cpu().numpy() for r in range(world)], axis=0)
+    blocks = allgather(local)
+    if len(blocks) != world:
+        raise ValueError(f"allgather returned {len(blocks)} blocks for {world} ranks")
+    return merge_rows(blocks, n_frames)
 
 
-def binding_frames_sharded(system, frames_f32_A, group=None) -> np.ndarray:
+def binding_frames_sharded(system, frames_f32_A, rank: int, world: int,
+                           allgather: Callable[[object], list]) -> np.ndarray:
     """(F, 13) frame energies of all F frames, each rank evaluating its range
     with ``system`` (a BindingSystem on that rank's GPU); every rank receives
     the full array."""
-    import torch.distributed as dist
-
     F = frames_f32_A.shape[0]
-    a, b = frame_range(F, dist.get_rank(group), dist.get_world_size(group))
+    a, b = frame_range(F, rank, world)
     local = system.run(frames_f32_A[a:b]) if b > a else np.zeros((0, 13))
-    return gather_rows(local, F, group)
+    return gather_rows(local, F, rank, world, allgather)
 
 
 def statistics(rows: np.ndarray) -> dict:
