@@ -318,6 +318,18 @@ rstg_status rstg_system_pb_stats(const rstg_system* s, double* stats8);
  * at most 60 % of the free memory and 64 GB, about 140 bytes per grid point
  * of the complex, receptor and ligand grids of a frame). */
 rstg_status rstg_system_set_pb_batch(rstg_system* s, int64_t frames);
+/* Stopping rule of the batched PB engine (no reference counterpart).
+ * rel_tol = 0 (default): the reference's schedule -- V-cycles until the
+ * absolute RMS residual is below PbParams.tolerance, at most
+ * clamp(max_iterations / 6, 1, 200) cycles, Chebyshev SOR after divergence
+ * (pb_solver.rs:1015-1167) -- whose result on large solvated grids is the
+ * iterate at the cycle cap.  rel_tol > 0: every grid (focusing coarse grids
+ * included) is solved to ||f - A phi|| <= rel_tol ||f - A phi_0|| in FP64
+ * by defect correction with FP32 V-cycles of a consistent multigrid
+ * (Gauss-Seidel smoothing, full-weighting restriction, series/parallel
+ * coarse dielectrics), which converges where the reference's V-cycle
+ * stalls; the cycle cap stays.  Applies to later runs. */
+rstg_status rstg_system_set_pb_convergence(rstg_system* s, double rel_tol);
 /* Profile mode of the batched PB engine (no reference counterpart): when on,
  * later runs launch the multigrid cycles without graph capture and time the
  * finest-level kernels with CUDA events.  rstg_system_pb_profile returns

@@ -89,6 +89,11 @@ struct PbParams {
   size_t max_iterations = 10000;
   double fillratio = 4.0;
   size_t fscale = 8;
+  // > 0: solve every grid to this relative FP64 residual instead of the
+  // reference's schedule (the converged answer, not the reference's iterate)
+  double converged_rel_tol = 0.0;
+  size_t converged_max_iter = 20000;
+  int converged_method = 0;  // 0 Jacobi-PCG, 1 flexible CG + V-cycle, 2 defect correction + V-cycle
 };
 
 struct MmEnergy {

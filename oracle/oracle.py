@@ -36,7 +36,8 @@ class PbP(C.Structure):
     _fields_ = [("grid_spacing", C.c_double), ("grid_buffer", C.c_double), ("solute_dielectric", C.c_double),
                 ("solvent_dielectric", C.c_double), ("salt", C.c_double), ("temperature", C.c_double),
                 ("probe", C.c_double), ("ion_radius", C.c_double), ("tolerance", C.c_double),
-                ("max_iterations", C.c_int64), ("fillratio", C.c_double), ("fscale", C.c_int64)]
+                ("max_iterations", C.c_int64), ("fillratio", C.c_double), ("fscale", C.c_int64),
+                ("converged_rel_tol", C.c_double), ("converged_method", C.c_int64)]
 
 
 class TopoDesc(C.Structure):
@@ -144,10 +145,14 @@ def sa_params(surface_tension=0.0072, offset=0.0, probe=1.4, n_points=480) -> Sa
 
 def pb_params(grid_spacing=0.5, grid_buffer=10.0, solute_dielectric=1.0, solvent_dielectric=80.0, salt=0.15,
               temperature=300.0, probe=1.4, ion_radius=2.0, tolerance=1e-6, max_iterations=10000,
-              fillratio=4.0, fscale=8) -> PbP:
-    """PbParams with the reference defaults (pb_energy.rs:49-66)."""
+              fillratio=4.0, fscale=8, converged_rel_tol=0.0, converged_method=0) -> PbP:
+    """PbParams with the reference defaults (pb_energy.rs:49-66).  With
+    converged_rel_tol > 0 every grid is solved to that relative FP64
+    residual instead of the reference's schedule: method 0 Jacobi-PCG,
+    1 flexible CG preconditioned by a consistent V-cycle, 2 defect
+    correction with that V-cycle."""
     return PbP(grid_spacing, grid_buffer, solute_dielectric, solvent_dielectric, salt, temperature, probe,
-               ion_radius, tolerance, max_iterations, fillratio, fscale)
+               ion_radius, tolerance, max_iterations, fillratio, fscale, converged_rel_tol, converged_method)
 
 
 class Topology:

@@ -409,6 +409,8 @@ struct orc_pb_params {
   int64_t max_iterations;
   double fillratio;
   int64_t fscale;
+  double converged_rel_tol;  // > 0: converged solves (not the reference's schedule)
+  int64_t converged_method;
 };
 // Flat topology description for hand-built topologies (the reference's
 // unit tests build AmberTopology structs directly).
@@ -488,6 +490,8 @@ static PbParams pbp(const orc_pb_params* p) {
   b.max_iterations = (size_t)p->max_iterations;
   b.fillratio = p->fillratio;
   b.fscale = (size_t)p->fscale;
+  b.converged_rel_tol = p->converged_rel_tol;
+  b.converged_method = (int)p->converged_method;
   return b;
 }
 static std::vector<V3> coords(const double* xyz, size_t n) {

@@ -587,6 +587,41 @@ static void coarsen(const double* f, const size_t* fd, double* c, const size_t* 
       }
 }
 
+// Coarse face dielectrics of the converged solves' multigrid (the reference
+// injects, pb_solver.rs:684-748): a coarse face spans two fine faces in
+// series along its axis (harmonic mean; equal values are copied) and, across
+// it, the fine faces of the 3 x 3 neighbouring lines in parallel (weights
+// 1-2-1 in each transverse direction, renormalised at the grid edge).
+static void coarsen_face(const double* f, const size_t* fd, double* c, const size_t* cd, int axis) {
+  long n[3] = {(long)fd[0], (long)fd[1], (long)fd[2]};
+  int t1 = (axis + 1) % 3, t2 = (axis + 2) % 3;
+  for (size_t cz = 0; cz < cd[2]; cz++)
+    for (size_t cy = 0; cy < cd[1]; cy++)
+      for (size_t cx = 0; cx < cd[0]; cx++) {
+        long b[3] = {std::min(2 * (long)cx, n[0] - 1), std::min(2 * (long)cy, n[1] - 1),
+                     std::min(2 * (long)cz, n[2] - 1)};
+        double sum = 0.0, ws = 0.0, first = 0.0;
+        bool same = true, any = false;
+        for (int u = -1; u <= 1; u++)
+          for (int v = -1; v <= 1; v++) {
+            long p[3] = {b[0], b[1], b[2]};
+            p[t1] += u;
+            p[t2] += v;
+            if (p[t1] < 0 || p[t1] >= n[t1] || p[t2] < 0 || p[t2] >= n[t2]) continue;
+            long q1[3] = {p[0], p[1], p[2]};
+            q1[axis] = std::min(p[axis] + 1, n[axis] - 1);
+            double e0 = f[p[0] + n[0] * (p[1] + n[1] * p[2])], e1 = f[q1[0] + n[0] * (q1[1] + n[1] * q1[2])];
+            if (!any) first = e0;
+            any = true;
+            same = same && e0 == first && e1 == first;
+            double w = (u == 0 ? 2.0 : 1.0) * (v == 0 ? 2.0 : 1.0);
+            sum += w * (e0 == e1 ? e0 : 2.0 / (1.0 / e0 + 1.0 / e1));
+            ws += w;
+          }
+        c[cx + cd[0] * (cy + cd[1] * cz)] = same ? first : sum / ws;
+      }
+}
+
 struct Level {
   size_t cd[3], fd[3];
   double ch[3];
@@ -595,7 +630,7 @@ struct Level {
 };
 
 // pb_solver.rs:776-836
-static std::vector<Level> build_levels(const Op& top, size_t min_size) {
+static std::vector<Level> build_levels(const Op& top, size_t min_size, bool series_parallel = false) {
   std::vector<Level> L;
   size_t d[3] = {top.d[0], top.d[1], top.d[2]};
   double h[3] = {top.h[0], top.h[1], top.h[2]};
@@ -614,11 +649,17 @@ static std::vector<Level> build_levels(const Op& top, size_t min_size) {
     lv.ey.resize(cn);
     lv.ez.resize(cn);
     lv.k2.resize(cn);
-    coarsen(ex, d, lv.ex.data(), lv.cd);
-    coarsen(ey, d, lv.ey.data(), lv.cd);
-    coarsen(ez, d, lv.ez.data(), lv.cd);
+    if (series_parallel) {
+      coarsen_face(ex, d, lv.ex.data(), lv.cd, 0);
+      coarsen_face(ey, d, lv.ey.data(), lv.cd, 1);
+      coarsen_face(ez, d, lv.ez.data(), lv.cd, 2);
+    } else {
+      coarsen(ex, d, lv.ex.data(), lv.cd);
+      coarsen(ey, d, lv.ey.data(), lv.cd);
+      coarsen(ez, d, lv.ez.data(), lv.cd);
+    }
     coarsen(k2, d, lv.k2.data(), lv.cd);
-    lv.omega = estimate_omega(lv.cd);
+    lv.omega = series_parallel ? 1.0 : estimate_omega(lv.cd);
     lv.fres.assign(fn, 0.0);
     lv.crhs.assign(cn, 0.0);
     lv.ccorr.assign(cn, 0.0);
@@ -638,7 +679,7 @@ static std::vector<Level> build_levels(const Op& top, size_t min_size) {
 
 // pb_solver.rs:842-939
 static void v_cycle(const Op& o, double* phi, const double* rho, double omega, Level* L, size_t nl, size_t pre,
-                    size_t post, double rhs_scale) {
+                    size_t post, double rhs_scale, double rscale = 0.25) {
   if (nl == 0) {
     sor_smooth(o, phi, rho, omega, 50, rhs_scale);
     return;
@@ -646,7 +687,7 @@ static void v_cycle(const Op& o, double* phi, const double* rho, double omega, L
   Level& lv = L[0];
   sor_smooth(o, phi, rho, omega, pre, rhs_scale);
   residual_into(o, phi, rho, rhs_scale, lv.fres.data());
-  restrict_into(lv.fres.data(), lv.fd, lv.crhs.data(), lv.cd, 0.25);
+  restrict_into(lv.fres.data(), lv.fd, lv.crhs.data(), lv.cd, rscale);
   std::fill(lv.ccorr.begin(), lv.ccorr.end(), 0.0);
   Op co;
   for (int k = 0; k < 3; k++) {
@@ -657,7 +698,7 @@ static void v_cycle(const Op& o, double* phi, const double* rho, double omega, L
   co.ey = lv.ey.data();
   co.ez = lv.ez.data();
   co.k2 = lv.k2.data();
-  v_cycle(co, lv.ccorr.data(), lv.crhs.data(), lv.omega, L + 1, nl - 1, pre, post, 1.0);
+  v_cycle(co, lv.ccorr.data(), lv.crhs.data(), lv.omega, L + 1, nl - 1, pre, post, 1.0, rscale);
   prolongate_add(lv.ccorr.data(), lv.cd, phi, o.d);
   sor_smooth(o, phi, rho, omega, post, rhs_scale);
 }
@@ -768,6 +809,163 @@ SolveResult solve_multigrid(const Grid& g, const std::vector<double>& rho, const
   return R;
 }
 
+// ---------------------------------------------------------------------------
+// Converged solves (not part of the reference's schedule).  The reference
+// stops its V-cycles on an absolute RMS residual or after at most 200 cycles
+// (pb_solver.rs:1066, 1093-1141); on solvated grids of realistic size that
+// cap is reached long before the discrete system is solved.  These solvers
+// give the converged solution of the same discrete system (same maps, same
+// boundary values, same 7-point operator), the error reference for solvers
+// that stop on a relative residual.  The interior unknowns solve A phi = f,
+// A = -div eps grad + kbar^2, symmetric positive definite (the face
+// dielectric between two points is one value used by both rows); boundary
+// values are fixed.  Relative residual = ||f - A phi||_2 / ||f - A phi_0||_2
+// over interior points, phi_0 = the initial potential (zero inside,
+// boundary values set).  The multigrid of methods 1 and 2 is a consistent
+// one, unlike the reference's: red-black Gauss-Seidel smoothing (omega 1,
+// 3 + 3 sweeps, 50 on the coarsest level), full-weighting restriction
+// without the 0.25 factor, series/parallel coarse dielectrics, kbar^2
+// injected, corrections zero on the boundary.
+//   method 0: conjugate gradients, diagonal (Jacobi) preconditioner --
+//             independent of any multigrid hierarchy;
+//   method 1: flexible conjugate gradients (Polak-Ribiere form) with one
+//             V-cycle on the residual equation as the preconditioner;
+//   method 2: defect correction phi += V-cycle(f - A phi), the iteration
+//             of the GPU engine's relative-residual mode, here in FP64.
+static double dot_int(const Op& o, const double* a, const double* b) {
+  size_t nx = o.d[0], ny = o.d[1], nz = o.d[2];
+  std::vector<double> part(nz, 0.0);
+#pragma omp parallel for schedule(static)
+  for (long izl = 1; izl < (long)nz - 1; izl++) {
+    size_t iz = (size_t)izl;
+    double s = 0.0;
+    for (size_t iy = 1; iy + 1 < ny; iy++)
+      for (size_t ix = 1; ix + 1 < nx; ix++) {
+        size_t idx = ix + nx * iy + nx * ny * iz;
+        s += a[idx] * b[idx];
+      }
+    part[iz] = s;
+  }
+  double s = 0.0;
+  for (double v : part) s += v;
+  return s;
+}
+
+// q = A v at interior points, v taken as zero on the boundary
+static void apply_op(const Op& o, const double* v, double* q) {
+  size_t nx = o.d[0], ny = o.d[1], nz = o.d[2];
+  double ihx = 1.0 / (o.h[0] * o.h[0]), ihy = 1.0 / (o.h[1] * o.h[1]), ihz = 1.0 / (o.h[2] * o.h[2]);
+#pragma omp parallel for schedule(static)
+  for (long izl = 1; izl < (long)nz - 1; izl++) {
+    size_t iz = (size_t)izl;
+    for (size_t iy = 1; iy + 1 < ny; iy++)
+      for (size_t ix = 1; ix + 1 < nx; ix++) {
+        size_t idx = ix + nx * iy + nx * ny * iz;
+        double ns, dg;
+        stencil(o, v, idx, ihx, ihy, ihz, ns, dg);
+        q[idx] = dg * v[idx] - ns;
+      }
+  }
+}
+
+static void zero_boundary(const Op& o, double* v) {
+  size_t nx = o.d[0], ny = o.d[1], nz = o.d[2];
+  for (size_t iz = 0; iz < nz; iz++)
+    for (size_t iy = 0; iy < ny; iy++)
+      for (size_t ix = 0; ix < nx; ix++)
+        if (ix == 0 || iy == 0 || iz == 0 || ix + 1 == nx || iy + 1 == ny || iz + 1 == nz)
+          v[ix + nx * iy + nx * ny * iz] = 0.0;
+}
+
+SolveResult solve_converged(const Grid& g, const std::vector<double>& rho, const Diel& D,
+                            const std::vector<double>& k2, const BC& bc, const std::vector<V3>& x,
+                            const std::vector<double>& q, double kb, double eout, double rel_tol, size_t maxit,
+                            int method) {
+  Op o;
+  for (int k = 0; k < 3; k++) {
+    o.d[k] = g.dims[k];
+    o.h[k] = g.h[k];
+  }
+  o.ex = D.ex.data();
+  o.ey = D.ey.data();
+  o.ez = D.ez.data();
+  o.k2 = k2.data();
+  SolveResult R;
+  R.phi.assign(g.len(), 0.0);
+  apply_bc(R.phi, g, bc, x, q, kb, eout);
+  size_t n = g.len();
+  std::vector<double> r(n, 0.0), z(n, 0.0), p(n, 0.0), Ap(n, 0.0), rold(n, 0.0), diag(n, 1.0);
+  residual_into(o, R.phi.data(), rho.data(), FOUR_PI_EC, r.data());
+  double r0 = std::sqrt(dot_int(o, r.data(), r.data()));
+  R.residual = r0 > 0.0 ? 1.0 : 0.0;
+  if (r0 == 0.0) {
+    R.converged = true;
+    return R;
+  }
+  size_t md = std::min(g.dims[0], std::min(g.dims[1], g.dims[2]));
+  bool mg = method >= 1 && md > 8;
+  std::vector<Level> L;
+  if (mg) L = build_levels(o, 5, true);
+  if (!mg) {
+    size_t nx = o.d[0], ny = o.d[1];
+    double ihx = 1.0 / (o.h[0] * o.h[0]), ihy = 1.0 / (o.h[1] * o.h[1]), ihz = 1.0 / (o.h[2] * o.h[2]);
+    for (size_t iz = 1; iz + 1 < o.d[2]; iz++)
+      for (size_t iy = 1; iy + 1 < ny; iy++)
+        for (size_t ix = 1; ix + 1 < nx; ix++) {
+          size_t idx = ix + nx * iy + nx * ny * iz;
+          double ns, dg;
+          stencil(o, R.phi.data(), idx, ihx, ihy, ihz, ns, dg);
+          diag[idx] = dg;
+        }
+  }
+  bool krylov = method != 2 || !mg;
+  double rz_old = 0.0;
+  for (size_t it = 0; it < maxit; it++) {
+    if (mg) {
+      std::fill(z.begin(), z.end(), 0.0);
+      v_cycle(o, z.data(), r.data(), 1.0, L.data(), L.size(), 3, 3, 1.0, 1.0);
+    } else {
+      for (size_t i = 0; i < n; i++) z[i] = r[i] / diag[i];
+    }
+    zero_boundary(o, z.data());
+    R.iterations = it + 1;
+    if (!krylov) {
+      for (size_t i = 0; i < n; i++) R.phi[i] += z[i];
+      residual_into(o, R.phi.data(), rho.data(), FOUR_PI_EC, r.data());
+    } else {
+      double rz = dot_int(o, r.data(), z.data());
+      if (it == 0) {
+        p = z;
+      } else {
+        // Polak-Ribiere: CG for a fixed symmetric preconditioner, stable for a
+        // variable or non-symmetric one (flexible CG)
+        double beta = (rz - dot_int(o, rold.data(), z.data())) / rz_old;
+        for (size_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+      }
+      apply_op(o, p.data(), Ap.data());
+      double alpha = rz / dot_int(o, p.data(), Ap.data());
+      rold = r;
+      for (size_t i = 0; i < n; i++) {
+        R.phi[i] += alpha * p[i];
+        r[i] -= alpha * Ap[i];
+      }
+      rz_old = rz;
+    }
+    double rel = std::sqrt(dot_int(o, r.data(), r.data())) / r0;
+    if (krylov && (rel < rel_tol || (it + 1) % 50 == 0)) {  // the recurrence drifts: true residual
+      residual_into(o, R.phi.data(), rho.data(), FOUR_PI_EC, r.data());
+      rel = std::sqrt(dot_int(o, r.data(), r.data())) / r0;
+    }
+    R.residual = rel;
+    if (!std::isfinite(rel)) break;
+    if (rel < rel_tol) {
+      R.converged = true;
+      return R;
+    }
+  }
+  return R;
+}
+
 // pb_solver.rs:1174-1186
 double elec_energy(const Grid& g, const std::vector<double>& phi, const std::vector<V3>& x,
                    const std::vector<double>& q) {
@@ -786,6 +984,13 @@ static double solve_focus(const Grid& fg, const std::vector<double>& fq, const G
   double bck = ionic ? kap : 0.0;
   BC dh;
   dh.kind = 1;
+  auto fine_solve = [&](const Grid& g, const std::vector<double>& rho, const Diel& D, const std::vector<double>& K,
+                        const BC& bc) {
+    if (p.converged_rel_tol > 0.0)
+      return solve_converged(g, rho, D, K, bc, x, q, bck, eout, p.converged_rel_tol, p.converged_max_iter,
+                             p.converged_method);
+    return solve_multigrid(g, rho, D, K, bc, x, q, bck, eout, p.tolerance, p.max_iterations);
+  };
   auto fine_maps = [&](Diel& D, std::vector<double>& K) {
     D = assign_dielectrics(fg, x, radii, p.probe, ein, eout);
     if (ionic)
@@ -798,7 +1003,10 @@ static double solve_focus(const Grid& fg, const std::vector<double>& fq, const G
     Diel cD = assign_dielectrics(*cg, x, radii, p.probe, ein, eout);
     std::vector<double> cK =
         ionic ? assign_kappa(*cg, x, radii, p.ion_radius, kap, p.solvent_dielectric) : std::vector<double>(cg->len(), 0.0);
-    SolveResult cr = solve_multigrid(*cg, cq, cD, cK, dh, x, q, bck, eout, p.tolerance * 10.0, p.max_iterations);
+    SolveResult cr = p.converged_rel_tol > 0.0
+                         ? solve_converged(*cg, cq, cD, cK, dh, x, q, bck, eout, p.converged_rel_tol,
+                                           p.converged_max_iter, p.converged_method)
+                         : solve_multigrid(*cg, cq, cD, cK, dh, x, q, bck, eout, p.tolerance * 10.0, p.max_iterations);
     double mp = 0.0;
     for (double v : cr.phi) mp = std::max(mp, std::fabs(v));
     bool ok = cr.converged && std::isfinite(mp) && mp < 1e10;
@@ -806,7 +1014,7 @@ static double solve_focus(const Grid& fg, const std::vector<double>& fq, const G
     std::vector<double> K;
     fine_maps(D, K);
     if (!ok) {
-      *out = solve_multigrid(fg, fq, D, K, dh, x, q, bck, eout, p.tolerance, p.max_iterations);
+      *out = fine_solve(fg, fq, D, K, dh);
       return elec_energy(fg, out->phi, x, q);
     }
     BC ib;
@@ -816,13 +1024,13 @@ static double solve_focus(const Grid& fg, const std::vector<double>& fq, const G
       fg.point(ix, iy, iz, pt);
       ib.values.push_back({fg.index(ix, iy, iz), interpolate(*cg, pt, cr.phi)});
     });
-    *out = solve_multigrid(fg, fq, D, K, ib, x, q, bck, eout, p.tolerance, p.max_iterations);
+    *out = fine_solve(fg, fq, D, K, ib);
     return elec_energy(fg, out->phi, x, q);
   }
   Diel D;
   std::vector<double> K;
   fine_maps(D, K);
-  *out = solve_multigrid(fg, fq, D, K, dh, x, q, bck, eout, p.tolerance, p.max_iterations);
+  *out = fine_solve(fg, fq, D, K, dh);
   return elec_energy(fg, out->phi, x, q);
 }
 

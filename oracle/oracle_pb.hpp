@@ -58,6 +58,14 @@ void prolongate_add(const double* coarse, const size_t* cd, double* fine, const 
 SolveResult solve_multigrid(const Grid& g, const std::vector<double>& rho, const Diel& D,
                             const std::vector<double>& k2, const BC& bc, const std::vector<V3>& x,
                             const std::vector<double>& q, double kb, double eout, double tol, size_t maxit);
+// Converged solve of the same discrete system to a relative residual
+// (method 0 Jacobi-preconditioned CG, 1 flexible CG with a consistent
+// V-cycle, 2 defect correction with that V-cycle); not the reference's
+// schedule.
+SolveResult solve_converged(const Grid& g, const std::vector<double>& rho, const Diel& D,
+                            const std::vector<double>& k2, const BC& bc, const std::vector<V3>& x,
+                            const std::vector<double>& q, double kb, double eout, double rel_tol, size_t maxit,
+                            int method);
 double elec_energy(const Grid& g, const std::vector<double>& phi, const std::vector<V3>& x,
                    const std::vector<double>& q);
 

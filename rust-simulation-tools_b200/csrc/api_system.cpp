@@ -239,6 +239,15 @@ rstg_status rstg_system_set_pb_batch(rstg_system* s, int64_t frames) {
   });
 }
 
+rstg_status rstg_system_set_pb_convergence(rstg_system* s, double rel_tol) {
+  return guard([&] {
+    if (!s) throw Error(RSTG_ERR_INVALID, "system must not be NULL");
+    if (!(rel_tol >= 0.0) || rel_tol >= 1.0) throw Error(RSTG_ERR_INVALID, "rel_tol must be in [0, 1)");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    s->pb_rel_tol = rel_tol;
+  });
+}
+
 rstg_status rstg_system_profile(rstg_system* s, const float* d_frames, int64_t F, int32_t* n, char* names,
                                 double* ms, double* flops, double* bytes) {
   return guard([&] {

@@ -19,6 +19,17 @@
 // the residual equation from e = 0 equals one sweep on phi, and the sweep's
 // update measure sum (gs - old)^2 is the same quantity.
 //
+// Relative-residual mode (PbJob::rtol > 0; not the reference's schedule):
+// the same FP64 defect correction, with a consistent multigrid as the FP32
+// inner solver -- red-black Gauss-Seidel sweeps (omega 1), full-weighting
+// restriction without the reference's 0.25 factor, series/parallel coarse
+// face dielectrics (k_coarsen32), corrections kept zero on the boundary --
+// and the stop when the FP64 residual norm falls below rtol times its
+// initial value.  The reference's V-cycle stalls on solvated grids (its
+// coarse correction is a quarter of the consistent one and its coarse
+// dielectrics are injected); this one reaches a 1e-6 relative residual in
+// about a dozen cycles on the 3,040-atom workload.
+//
 // Launches are driven by work lists: for each launch the host lists the
 // grids that take part and the first block of each, so no block is spent on
 // a grid that has finished or is smaller than the largest one.  The lists
@@ -78,6 +89,7 @@ struct JobD {
   double ih, eps, tol, rs2;
   double ox, oy, oz, h;
   long long maxit;
+  double rtol;  // > 0: stop on the relative FP64 residual (consistent multigrid)
 };
 
 struct LvlD {
@@ -85,8 +97,9 @@ struct LvlD {
   const float *ex, *ey, *ez, *k2;
   const uint8_t* cd;          // stencil codes
   int nx, ny, nz, uniform;
-  int px, zc, pad1, pad2;     // row pitch (nx rounded up to 4: rows start on 16-byte boundaries), sweep z chunk
-  float ih, om, eps, pad;
+  int px, zc, skipb, pad2;    // row pitch (nx rounded up to 4: rows start on 16-byte boundaries), sweep z chunk,
+                              // skipb: prolongation leaves boundary points alone (relative-residual mode)
+  float ih, om, eps, rsc;     // rsc: restriction scale (0.25 the reference's, 1 relative-residual mode)
   float fin, fout, kb, pad3;
 };
 
@@ -310,10 +323,10 @@ __global__ void __launch_bounds__(256, 4) k_upres64(WL w, const JobD* __restrict
 // RMS of the residual and the reference's multigrid bookkeeping
 // (pb_solver.rs:1080-1160); one block per listed grid.
 __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ S, const double* __restrict__ part,
-                       int nparts, int check) {
+                       int nparts, int check, int want) {
   __shared__ double sh[32];
   int j = w.job[blockIdx.x];
-  if (S[j].status != kMg) return;
+  if (S[j].status != want) return;
   const JobD& d = J[j];
   int used = ((d.nx + 31) >> 5) * ((d.ny + 7) >> 3) * ((d.nz + 7) >> 3);
   double s = 0.0;
@@ -342,7 +355,7 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
     return;
   }
   t.prev = r;
-  if (r < d.tol) {
+  if (d.rtol > 0.0 ? r < d.rtol * t.r0 : r < d.tol) {
     t.status = kConverged;
   } else if (t.cycles >= d.maxv) {
     t.status = kMgCap;
@@ -624,15 +637,20 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
 // of the sweep's updates from the sweep blocks' partial sums (fixed order),
 // Chebyshev omega for the next sweep, convergence; k_upres64 wrote the new
 // potential into the other buffer.
+// In relative-residual mode the test is on the FP64 residual of the new
+// potential (k_upres64's per-brick sums in rpart) against the initial one.
 __global__ void k_sor_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ S, const double* __restrict__ part,
-                           int nparts) {
+                           const double* __restrict__ rpart, int nparts) {
   __shared__ double sh[32];
   int j = w.job[blockIdx.x];
   if (S[j].status != kSor) return;
   const JobD& d = J[j];
-  const int used = ((d.nx + kSwTX - 1) / kSwTX) * ((d.ny + kSwTY - 1) / kSwTY) * ((d.nz + kSwZC0 - 1) / kSwZC0);
+  const bool rel = d.rtol > 0.0;
+  const int used = rel ? ((d.nx + 31) >> 5) * ((d.ny + 7) >> 3) * ((d.nz + 7) >> 3)
+                       : ((d.nx + kSwTX - 1) / kSwTX) * ((d.ny + kSwTY - 1) / kSwTY) * ((d.nz + kSwZC0 - 1) / kSwZC0);
+  const double* src = rel ? rpart : part;
   double s = 0.0;
-  for (int k = threadIdx.x; k < used; k += blockDim.x) s += part[(long long)j * nparts + k];
+  for (int k = threadIdx.x; k < used; k += blockDim.x) s += src[(long long)j * nparts + k];
   s = block_sum(s, sh);
   if (threadIdx.x != 0) return;
   double cnt = (double)(d.nx - 2) * (double)(d.ny - 2) * (double)(d.nz - 2);
@@ -643,7 +661,7 @@ __global__ void k_sor_norm(WL w, const JobD* __restrict__ J, JobState* __restric
   t.rms = rms;
   t.sor_it = it + 1;
   t.om = it == 0 ? 1.0 / (1.0 - d.rs2 / 2.0) : 1.0 / (1.0 - d.rs2 * t.om / 4.0);
-  if (rms < d.tol)
+  if (rel ? rms < d.rtol * t.r0 : rms < d.tol)
     t.status = kConverged;
   else if (t.sor_it >= d.maxit)
     t.status = kSorCap;
@@ -670,7 +688,8 @@ __global__ void __launch_bounds__(256) k_res32(WL w, const LvlD* __restrict__ L,
   }
 }
 
-// Full-weighting restriction x 0.25 of the level-l residual into the
+// Full-weighting restriction (x 0.25 in the reference's schedule, x 1 in the
+// relative-residual mode) of the level-l residual into the
 // level-(l+1) right-hand side (pb_solver.rs:459-520); the coarse correction
 // starts from zero.
 __global__ void __launch_bounds__(256) k_restrict32(WL w, const LvlD* __restrict__ L, int lvl,
@@ -678,6 +697,7 @@ __global__ void __launch_bounds__(256) k_restrict32(WL w, const LvlD* __restrict
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != kMg) return;
   const Lv f = lv_load(L, j, lvl), c = lv_load(L, j, lvl + 1);
+  const float rsc = L[j * kMaxLev + lvl].rsc;
   int cx, cy, cz0;
   brick_col(lb, c.nx, c.ny, cx, cy, cz0);
   if (cx >= c.nx || cy >= c.ny) return;
@@ -706,22 +726,25 @@ __global__ void __launch_bounds__(256) k_restrict32(WL w, const LvlD* __restrict
       }
     }
     int i = cx + c.sy * cy + c.sz * cz;
-    c.rhs[i] = 0.25f * sum / ws;
+    c.rhs[i] = rsc * sum / ws;
     c.e[i] = 0.0f;
   }
 }
 
 // Trilinear prolongation of the level-(l+1) correction added at every
-// level-l point (pb_solver.rs:522-578); the fine correction is in e2 between
+// level-l point (pb_solver.rs:522-578; interior points only in the
+// relative-residual mode, where corrections vanish on the boundary); the fine correction is in e2 between
 // the pre- and post-smoothing sweeps, the coarse one in e.
 __global__ void __launch_bounds__(256) k_prolong32(WL w, const LvlD* __restrict__ L, int lvl,
                                                    const JobState* __restrict__ S) {
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != kMg) return;
   const Lv f = lv_load(L, j, lvl), c = lv_load(L, j, lvl + 1);
+  const bool skipb = L[j * kMaxLev + lvl].skipb != 0;
   int fx, fy, fz0;
   brick_col(lb, f.nx, f.ny, fx, fy, fz0);
   if (fx >= f.nx || fy >= f.ny) return;
+  if (skipb && (fx == 0 || fx == f.nx - 1 || fy == 0 || fy == f.ny - 1)) return;
   const float* __restrict__ ce = c.e;
   int mx = c.nx >= 2 ? c.nx - 2 : 0, my = c.ny >= 2 ? c.ny - 2 : 0, mz = c.nz >= 2 ? c.nz - 2 : 0;
   int x0 = min(fx >> 1, mx), y0 = min(fy >> 1, my);
@@ -729,7 +752,7 @@ __global__ void __launch_bounds__(256) k_prolong32(WL w, const LvlD* __restrict_
 #pragma unroll
   for (int k = 0; k < 8; k++) {
     int fz = fz0 + k;
-    if (fz >= f.nz) continue;
+    if (fz >= f.nz || (skipb && (fz == 0 || fz == f.nz - 1))) continue;
     int z0 = min(fz >> 1, mz);
     float dz = (float)fz * 0.5f - (float)z0;
     const float* b = ce + x0 + c.sy * y0 + c.sz * z0;
@@ -927,6 +950,60 @@ __global__ void k_inject32(WL w, const LvlD* __restrict__ L, int lvl) {
   ((float*)c.ez)[ci] = f.ez[fi];
   ((float*)c.k2)[ci] = f.k2[fi];
   ((uint8_t*)c.cd)[ci] = f.cd[fi] & 127u;  // maps are injected, so are their codes; no rho below level 0
+}
+
+// Coarse maps of the relative-residual mode: a coarse face spans two fine
+// faces in series along its axis (harmonic mean, equal values copied) and
+// the fine faces of the 3 x 3 neighbouring lines across it in parallel
+// (weights 1-2-1 per transverse direction, renormalised at the grid edge);
+// kbar^2 and its code bit are injected.  Face codes by exact compares, as at
+// level 0 (a face whose lines are all eps_in is eps_in exactly).
+__device__ __forceinline__ float coarse_face(const LvlD& f, const float* __restrict__ m, int axis, int bx, int by,
+                                             int bz) {
+  const int n[3] = {f.nx, f.ny, f.nz};
+  const int t1 = axis == 0 ? 1 : 0, t2 = axis == 2 ? 1 : 2;
+  float sum = 0.0f, ws = 0.0f, first = 0.0f;
+  bool same = true, any = false;
+  for (int u = -1; u <= 1; u++)
+    for (int v = -1; v <= 1; v++) {
+      int p[3] = {bx, by, bz};
+      p[t1] += u;
+      p[t2] += v;
+      if (p[t1] < 0 || p[t1] >= n[t1] || p[t2] < 0 || p[t2] >= n[t2]) continue;
+      int q[3] = {p[0], p[1], p[2]};
+      q[axis] = min(p[axis] + 1, n[axis] - 1);
+      const float e0 = m[p[0] + f.px * (p[1] + f.ny * p[2])], e1 = m[q[0] + f.px * (q[1] + f.ny * q[2])];
+      if (!any) first = e0;
+      any = true;
+      same = same && e0 == first && e1 == first;
+      const float w = (u == 0 ? 2.0f : 1.0f) * (v == 0 ? 2.0f : 1.0f);
+      sum += w * (e0 == e1 ? e0 : 2.0f / (1.0f / e0 + 1.0f / e1));
+      ws += w;
+    }
+  return same ? first : sum / ws;
+}
+__device__ __forceinline__ unsigned fcode32(float v, float ein, float eout) {
+  return v == eout ? 0u : (v == ein ? 1u : 2u);
+}
+__global__ void k_coarsen32(WL w, const LvlD* __restrict__ L, int lvl) {
+  int lb, j = wl_job(w, blockIdx.x, lb);
+  const LvlD& f = L[j * kMaxLev + lvl];
+  const LvlD& c = L[j * kMaxLev + lvl + 1];
+  int cn = c.nx * c.ny * c.nz;
+  int i = lb * blockDim.x + threadIdx.x;
+  if (i >= cn) return;
+  int cx = i % c.nx, cy = (i / c.nx) % c.ny, cz = i / (c.nx * c.ny);
+  int bx = min(2 * cx, f.nx - 1), by = min(2 * cy, f.ny - 1), bz = min(2 * cz, f.nz - 1);
+  int fi = bx + f.px * (by + f.ny * bz);
+  int ci = cx + c.px * (cy + c.ny * cz);
+  const float ex = coarse_face(f, f.ex, 0, bx, by, bz), ey = coarse_face(f, f.ey, 1, bx, by, bz),
+              ez = coarse_face(f, f.ez, 2, bx, by, bz);
+  ((float*)c.ex)[ci] = ex;
+  ((float*)c.ey)[ci] = ey;
+  ((float*)c.ez)[ci] = ez;
+  ((float*)c.k2)[ci] = f.k2[fi];
+  ((uint8_t*)c.cd)[ci] = (uint8_t)(fcode32(ex, c.fin, c.fout) | (fcode32(ey, c.fin, c.fout) << 2) |
+                                   (fcode32(ez, c.fin, c.fout) << 4) | (f.cd[fi] & 64u));
 }
 
 // 0.5 sum_a q_a phi(x_a), trilinear phi (pb_solver.rs:1174-1186); one block per grid.
@@ -1220,6 +1297,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     d.tol = J.tol;
     d.maxv = (int)std::min<int64_t>(std::max<int64_t>(J.maxit / 6, 1), 200);
     d.maxit = J.maxit;
+    d.rtol = J.rtol > 0.0 ? J.rtol : 0.0;
     double rj = (std::cos(kPi / (double)J.g.nx) + std::cos(kPi / (double)J.g.ny) + std::cos(kPi / (double)J.g.nz)) / 3.0;
     d.rs2 = rj * rj;  // spectral radius of Jacobi, squared (pb_solver.rs:387-392)
     d.axyz = J.atoms->xyz.as<double>();
@@ -1261,12 +1339,14 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       L.fin = (float)J.ein;
       L.fout = (float)J.eout;
       L.kb = (float)d.dkb;
+      L.rsc = J.rtol > 0.0 ? 1.0f : 0.25f;
+      L.skipb = J.rtol > 0.0 ? 1 : 0;
       L.nx = g.nx;
       L.ny = g.ny;
       L.nz = g.nz;
       L.uniform = J.uniform ? 1 : 0;
       L.ih = (float)(1.0 / (g.h * g.h));
-      L.om = (float)pb_omega(g.nx, g.ny, g.nz);
+      L.om = J.rtol > 0.0 ? 1.0f : (float)pb_omega(g.nx, g.ny, g.nz);
       L.eps = (float)J.ein;
     }
   }
@@ -1290,14 +1370,18 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   {
     Lists setup;
     int s0 = setup.add_slot(), sc = setup.add_slot();
-    std::vector<int> si(kMaxLev);
-    for (int l = 0; l + 1 < kMaxLev; l++) si[l] = setup.add_slot();
+    std::vector<int> si(kMaxLev), sv(kMaxLev);
+    for (int l = 0; l + 1 < kMaxLev; l++) {
+      si[l] = setup.add_slot();
+      sv[l] = setup.add_slot();
+    }
     int maxl = 0;
     for (int j = 0; j < nj; j++) {
       setup.add(sc, j, cdiv((long long)jobs[j].g.n(), kT));
       if (jobs[j].uniform) continue;
       setup.add(s0, j, cdiv((long long)jobs[j].g.n(), kT));
-      for (int l = 0; l < lay[j].nlev; l++) setup.add(si[l], j, cdiv((long long)lay[j].lv[l + 1].n(), kT));
+      for (int l = 0; l < lay[j].nlev; l++)
+        setup.add(jobs[j].rtol > 0.0 ? sv[l] : si[l], j, cdiv((long long)lay[j].lv[l + 1].n(), kT));
       maxl = std::max(maxl, lay[j].nlev);
     }
     std::vector<WL> wl;
@@ -1311,11 +1395,16 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       k_maps32<<<setup.slots[s0].total, kT, 0, st>>>(wl[s0], dJ, dL);
       launched(c_);
     }
-    for (int l = 0; l < maxl; l++)
+    for (int l = 0; l < maxl; l++) {
       if (setup.slots[si[l]].total > 0) {
         k_inject32<<<setup.slots[si[l]].total, kT, 0, st>>>(wl[si[l]], dL, l);
         launched(c_);
       }
+      if (setup.slots[sv[l]].total > 0) {
+        k_coarsen32<<<setup.slots[sv[l]].total, kT, 0, st>>>(wl[sv[l]], dL, l);
+        launched(c_);
+      }
+    }
     int bad = 0;
     RSTG_CUDA(cudaMemcpyAsync(counts.data(), dcnt, 16 * (size_t)nj, cudaMemcpyDeviceToHost, st));
     RSTG_CUDA(cudaMemcpyAsync(&bad, dbad, 4, cudaMemcpyDeviceToHost, st));
@@ -1355,10 +1444,21 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       std::vector<WL> wl;
       init.upload(lists_, st, wl);
       k_res64<<<init.slots[s].total, kT, 0, st>>>(wl[s], dJ, dL, dS, kMg, part, nparts);
-      k_norm<<<init.slots[sn].total, 256, 0, st>>>(wl[sn], dJ, dS, part, nparts, 0);
+      k_norm<<<init.slots[sn].total, 256, 0, st>>>(wl[sn], dJ, dS, part, nparts, 0, kMg);
       launched(c_, 2);
     }
     sor_residuals(sor0);
+    // relative-residual SOR grids keep their initial residual norm as r0
+    Lists r0l;
+    int s0 = r0l.add_slot();
+    for (int j : sor0)
+      if (jobs[j].rtol > 0.0) r0l.add(s0, j, 1);
+    if (r0l.slots[s0].total > 0) {
+      std::vector<WL> wl;
+      r0l.upload(lists_, st, wl);
+      k_norm<<<r0l.slots[s0].total, 256, 0, st>>>(wl[s0], dJ, dS, part, nparts, 0, kSor);
+      launched(c_);
+    }
     RSTG_CUDA(cudaStreamSynchronize(st));
   }
   const int K = std::max(1, chunk_cycles), KS = 4;  // cycles per chunk, SOR sweeps per cycle
@@ -1443,7 +1543,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           sweeps(l, 1);
         }
         mark(2, dRes64, 0, [&] { k_upres64<<<go(s_res), kT, 0, st>>>(wl[s_res], dJ, dL, dS, kMg, part, nparts); });
-        mark(-1, dNorm, 0, [&] { k_norm<<<go(s_norm), 256, 0, st>>>(wl[s_norm], dJ, dS, part, nparts, 1); });
+        mark(-1, dNorm, 0, [&] { k_norm<<<go(s_norm), 256, 0, st>>>(wl[s_norm], dJ, dS, part, nparts, 1, kMg); });
         n += 3;
       }
       if (any_sor)
@@ -1453,7 +1553,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
           mark(-1, dSor, 0, [&] {
             k_sweep_t<true><<<go(s_sor), kSwThreads, sizeof(SwSmem), st>>>(wl[s_sor], dL, 0, dS, 1, 1, spart, nparts);
             k_upres64<<<go(s_sres), kT, 0, st>>>(wl[s_sres], dJ, dL, dS, kSor, part, nparts);
-            k_sor_norm<<<go(s_snorm), 256, 0, st>>>(wl[s_snorm], dJ, dS, spart, nparts);
+            k_sor_norm<<<go(s_snorm), 256, 0, st>>>(wl[s_snorm], dJ, dS, spart, part, nparts);
           });
           n += 3;
         }
@@ -1610,7 +1710,8 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     bool sor = s.status == kSorCap || s.sor_it > 0;
     jobs[j].fallback = sor;
     if (sor) stats.fallbacks++;
-    jobs[j].stats = PbSolveStats{sor ? (int64_t)s.sor_it : (int64_t)s.cycles, s.rms, s.status == kConverged};
+    double res = jobs[j].rtol > 0.0 ? (s.r0 > 0.0 ? s.rms / s.r0 : 0.0) : s.rms;  // relative in that mode
+    jobs[j].stats = PbSolveStats{sor ? (int64_t)s.sor_it : (int64_t)s.cycles, res, s.status == kConverged};
   }
   for (int j = 0; j < nj; j++) {  // the energy kernels read JobD::phi: point it at the current buffer
     phi_now[j] = hs[j].cur ? hd[j].phi2 : hd[j].phi;
@@ -1638,7 +1739,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
 
 void pb_polar_batch(Ctx* c, cudaStream_t st, PbBatchEngine& eng, const rstg_pb_params& p,
                     const std::vector<const std::vector<double>*>& xyz, const std::vector<const std::vector<double>*>& q,
-                    const std::vector<const std::vector<double>*>& r, double* out, rstg_pb_diag* diag) {
+                    const std::vector<const std::vector<double>*>& r, double* out, rstg_pb_diag* diag, double rtol) {
   if (!(p.grid_spacing > 0.0)) throw Error(RSTG_ERR_INVALID, "grid_spacing must be positive");
   PbStreamScope scope(st);
   size_t n = xyz.size();
@@ -1669,6 +1770,7 @@ void pb_polar_batch(Ctx* c, cudaStream_t st, PbBatchEngine& eng, const rstg_pb_p
     J.bc.eout = J.eout;
     J.tol = p.tolerance;
     J.maxit = p.max_iterations;
+    J.rtol = rtol;
     return J;
   };
   std::vector<DevBuf> cphi(2 * n);

@@ -17,6 +17,7 @@ struct PbJob {
   BcSpec bc;             // Debye-Hueckel, or interpolated from bc.cphi on *bc.cg
   double tol = 1e-6;
   int64_t maxit = 10000;
+  double rtol = 0.0;     // > 0: consistent multigrid, stop on this relative FP64 residual (not the reference's rule)
   bool energy = true;    // 0.5 sum q phi(atom) wanted
   int rho_of = -1;       // index of an earlier job of the batch with the same grid and atoms: use its charge map
   // results
@@ -76,8 +77,12 @@ class PbBatchEngine {
 // Polar PB energies (E_solvated - E_reference, pb_energy.rs:332-438) of
 // n_sets atom sets, batched.  xyz[i]: host Angstrom coordinates; q in e.
 // out[i] receives the energy, diag[i] (optional) the solve statistics.
+// rtol > 0 solves every grid (focusing coarse grids included) to that
+// relative FP64 residual with the consistent multigrid instead of the
+// reference's schedule.
 void pb_polar_batch(Ctx* c, cudaStream_t st, PbBatchEngine& eng, const rstg_pb_params& p,
                     const std::vector<const std::vector<double>*>& xyz, const std::vector<const std::vector<double>*>& q,
-                    const std::vector<const std::vector<double>*>& r, double* out, rstg_pb_diag* diag);
+                    const std::vector<const std::vector<double>*>& r, double* out, rstg_pb_diag* diag,
+                    double rtol = 0.0);
 
 }  // namespace rstg

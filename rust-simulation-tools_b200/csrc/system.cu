@@ -1460,7 +1460,7 @@ void System::run_pb(const void* frames, bool f64, bool host_in, int64_t F, rstg_
       }
     }
     pol.assign(B * 3, 0.0);
-    pb_polar_batch(ctx, st, *pbe, solv.pb, X, Q, R, pol.data(), nullptr);
+    pb_polar_batch(ctx, st, *pbe, solv.pb, X, Q, R, pol.data(), nullptr, pb_rel_tol);
     for (int64_t b = 0; b < B; b++) {
       rstg_frame_energy& e = res[f0 + b];
       e.complex.polar = pol[3 * b];

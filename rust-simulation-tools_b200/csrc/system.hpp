@@ -51,6 +51,7 @@ struct System {
   std::unique_ptr<PbBatchEngine> pbe;
   int64_t pb_frames_per_batch = 0;  // 0: from the device memory budget
   bool pb_profile = false;          // time the level-0 PB kernels
+  double pb_rel_tol = 0.0;          // > 0: PB grids solved to this relative residual (not the reference's rule)
 
   System(Ctx* c, const Topology& t, const std::vector<int64_t>& rres, const std::vector<int64_t>& lres,
          const rstg_solvation& s, const rstg_sa_params& sa, const rstg_system_opts& o);

@@ -788,6 +788,14 @@ class BindingSystem:
         names = ("sweep", "residual32", "residual64")
         return {n: {"ms": st[k], "bytes": st[4 + k], "launches": int(st[8 + k])} for k, n in enumerate(names)}
 
+    def set_pb_convergence(self, rel_tol: float = 0.0) -> None:
+        """PB stopping rule of later runs: 0 keeps the reference's schedule
+        (absolute RMS below ``PbParams.tolerance`` or the 200-cycle cap);
+        ``rel_tol`` > 0 solves every grid to that relative FP64 residual
+        with FP32 V-cycles of a consistent multigrid under FP64 defect
+        correction."""
+        check(N.lib.rstg_system_set_pb_convergence(self._h, float(rel_tol)))
+
     def set_pb_batch(self, frames: int) -> None:
         """Frames per batched PB launch sequence (0: from the memory budget)."""
         check(N.lib.rstg_system_set_pb_batch(self._h, int(frames)))

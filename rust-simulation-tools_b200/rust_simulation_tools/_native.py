@@ -145,6 +145,7 @@ _sig("rstg_system_last_stats", C.c_int, vp, ip)
 _sig("rstg_system_pb_stats", C.c_int, vp, dp)
 _sig("rstg_system_set_pb_batch", C.c_int, vp, i64)
 _sig("rstg_system_set_pb_profile", C.c_int, vp, i32)
+_sig("rstg_system_set_pb_convergence", C.c_int, vp, dbl)
 _sig("rstg_system_pb_profile", C.c_int, vp, dp)
 _sig("rstg_system_profile", C.c_int, vp, vp, i64, P(i32), C.c_char_p, dp, dp, dp)
 _sig("rstg_calibrate", C.c_int, C.c_int, dp)

@@ -1,0 +1,188 @@
+"""Parity at the benchmark configurations, against committed golden fixtures.
+
+tests/golden/cfg*.json hold the CPU restatement's results (oracle/) for
+frames of the seeded synthetic workloads at their full atom counts and grid
+sizes, written by tests/golden/make_golden.py; the digests in each file pin
+the generated inputs.  Tolerances:
+  * plain FP64 GPU form vs the faithful rows: sub-system terms relative
+    1e-10 (GB) and 1e-8 (PB, identical cycle counts); binding terms to the
+    same relative accuracy of the sub-system magnitudes (the reference forms
+    them as differences of totals);
+  * fused mixed-precision engine vs the accurate rows (exact binding
+    differences, FP64 reductions): binding terms within 1e-3 kcal/mol,
+    per-residue terms within 1e-4 kcal/mol;
+  * batched PB on the reference's schedule vs the faithful rows (the
+    reference's own iterate: absolute-RMS stop, 200-cycle cap, SOR after
+    divergence): polar terms within 1e-3 kcal/mol;
+  * batched PB with the relative-residual stop vs the converged rows (every
+    grid solved to a 1e-10 relative residual): polar terms within 1e-3.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+PB = {3: dict(grid_spacing=0.5, grid_buffer=12.0, fillratio=0.0), 5: dict(grid_spacing=0.5, grid_buffer=11.2, fillratio=0.0)}
+# relative FP64 residual at which the batched PB engine's converged polar
+# terms stay within 1e-3 kcal/mol of the 1e-10 solution on these grids
+PB_REL_TOL = 1e-8
+NPTS = 960
+
+
+def fixture(k):
+    with open(os.path.join(GOLDEN, f"cfg{k}.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="module")
+def inputs(tmp_path_factory):
+    """(system, frames, prmtop) of workload k, checked against the fixture's digests."""
+    from rust_simulation_tools import synthetic as S
+
+    cache = {}
+
+    def get(k):
+        if k not in cache:
+            fx = fixture(k)
+            s, fr = S.workload(k, n_frames=fx["frames"])
+            prm = str(tmp_path_factory.mktemp(f"cfg{k}") / f"w{k}.prmtop")
+            S.write_prmtop(s, prm)
+            assert hashlib.sha256(np.ascontiguousarray(fr, np.float32).tobytes()).hexdigest() == \
+                fx["inputs"]["frames_sha256"], "generated frames differ from the fixture's"
+            assert hashlib.sha256(open(prm, "rb").read()).hexdigest() == fx["inputs"]["prmtop_sha256"], \
+                "generated topology differs from the fixture's"
+            cache[k] = (s, fr, prm, fx)
+        return cache[k]
+
+    return get
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 5])
+def test_fixture_inputs_reproduce(inputs, k):
+    s, fr, _, fx = inputs(k)
+    assert fr.shape[0] == fx["frames"] and s.n_rec == fx["n_receptor_atoms"] and s.n_lig == fx["n_ligand_atoms"]
+
+
+def test_oracle_reproduces_cfg1_frame(inputs, oracle):
+    s, fr, prm, fx = inputs(1)
+    top = oracle.Topology.load(prm)
+    x = (fr[:1].astype(np.float64) * 0.1) * 10.0
+    gb, sa = oracle.gb_params("obc2", solvent_dielectric=78.5), oracle.sa_params(n_points=NPTS)
+    for acc, key in ((False, "gb_faithful"), (True, "gb_accurate")):
+        got = oracle.binding_frames(top, x, s.receptor_residues, s.ligand_residues, gb=gb, sa=sa, accurate=acc)
+        np.testing.assert_allclose(got[0], fx[key][0], rtol=1e-12, atol=1e-9)
+
+
+# --------------------------------------------------------------------------- GPU
+def _rst():
+    import rust_simulation_tools as r
+
+    if r.device_count() < 1:
+        pytest.skip("no CUDA device")
+    return r
+
+
+def _gb_system(rst, s, prm, mode):
+    top = rst.read_prmtop(prm)
+    return rst.BindingSystem(top, s.receptor_residues, s.ligand_residues,
+                             gb_params=rst.GbParams(model=rst.GbModel.ObcII, solvent_dielectric=78.5),
+                             sa_params=rst.SaParams(n_sphere_points=NPTS), mode=mode)
+
+
+def _pb_system(rst, s, prm, k, mode="fused"):
+    top = rst.read_prmtop(prm)
+    return rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, pb_params=rst.PbParams(**PB[k]),
+                             sa_params=rst.SaParams(n_sphere_points=NPTS), mode=mode)
+
+
+def _plain_vs_faithful(out, ref, rtol):
+    ref = np.asarray(ref)
+    scale = np.abs(ref[:, :9]).max(axis=1)
+    np.testing.assert_allclose(out[:, :9], ref[:, :9], rtol=rtol, atol=1e-9)
+    for k in (9, 10, 11, 12):
+        assert np.all(np.abs(out[:, k] - ref[:, k]) <= rtol * np.maximum(scale, 1.0)), k
+
+
+def _binding_terms(out, ref, cols=(9, 10, 11, 12), tol=1e-3):
+    ref = np.asarray(ref)
+    err = np.abs(out[:, list(cols)] - ref[:, list(cols)])
+    assert err.max() < tol, (err.max(axis=0), cols)
+    return float(err.max())
+
+
+@pytest.mark.gpu
+def test_cfg1_plain_all_frames(inputs):
+    rst = _rst()
+    s, fr, prm, fx = inputs(1)
+    out = _gb_system(rst, s, prm, "plain").run(fr)
+    _plain_vs_faithful(out, fx["gb_faithful"], 1e-10)
+
+
+@pytest.mark.gpu
+def test_cfg1_fused_all_frames(inputs):
+    rst = _rst()
+    s, fr, prm, fx = inputs(1)
+    out = _gb_system(rst, s, prm, "fused").run(fr)
+    _binding_terms(out, fx["gb_accurate"])
+    np.testing.assert_allclose(out[:, :9], np.asarray(fx["gb_accurate"])[:, :9], rtol=1e-6)
+
+
+@pytest.mark.gpu
+def test_cfg2_fused_with_decomposition(inputs):
+    rst = _rst()
+    s, fr, prm, fx = inputs(2)
+    out, dec = _gb_system(rst, s, prm, "fused").run(fr, decompose=True)
+    _binding_terms(out, fx["gb_accurate"])
+    np.testing.assert_allclose(out[:, :9], np.asarray(fx["gb_accurate"])[:, :9], rtol=1e-6)
+    np.testing.assert_allclose(dec, np.asarray(fx["decomposition_accurate"]), rtol=0, atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_cfg2_plain_frame(inputs):
+    rst = _rst()
+    s, fr, prm, fx = inputs(2)
+    out = _gb_system(rst, s, prm, "plain").run(fr[:1])
+    _plain_vs_faithful(out, fx["gb_faithful"][:1], 1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [3, 5])
+def test_pb_reference_schedule(inputs, k):
+    rst = _rst()
+    s, fr, prm, fx = inputs(k)
+    out = _pb_system(rst, s, prm, k).run(fr)
+    _binding_terms(out, fx["pb_faithful"], cols=(1, 4, 7, 10))
+    _binding_terms(out, fx["pb_converged"], cols=(9, 11))  # MM and SA binding terms: exact differences
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [3, 5])
+def test_pb_relative_residual(inputs, k):
+    rst = _rst()
+    s, fr, prm, fx = inputs(k)
+    sysf = _pb_system(rst, s, prm, k)
+    sysf.set_pb_convergence(PB_REL_TOL)
+    out = sysf.run(fr)
+    _binding_terms(out, fx["pb_converged"], cols=(1, 4, 7, 9, 10, 11, 12))
+
+
+@pytest.mark.gpu
+def test_cfg3_plain_pb_frame(inputs):
+    rst = _rst()
+    s, fr, prm, fx = inputs(3)
+    out = _pb_system(rst, s, prm, 3, mode="plain").run(fr[:1])
+    ref = np.asarray(fx["pb_faithful"])[:1]
+    np.testing.assert_allclose(out[:, [1, 4, 7]], ref[:, [1, 4, 7]], rtol=1e-8)
+
+
+@pytest.mark.gpu
+def test_cfg5_gb_frame(inputs):
+    rst = _rst()
+    s, fr, prm, fx = inputs(5)
+    out = _gb_system(rst, s, prm, "fused").run(fr)
+    _binding_terms(out, fx["gb_accurate"])
+    plain = _gb_system(rst, s, prm, "plain").run(fr)
+    _plain_vs_faithful(plain, fx["gb_faithful"], 1e-10)
