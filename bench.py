@@ -195,10 +195,30 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
-def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs):
-    """MM-PBSA frames/s, batched mixed precision vs plain FP64 on the same frames
-    (per-frame solve cost varies: some frames stop at the cycle cap, some
-    diverge and finish with SOR)."""
+def _golden(k):
+    """Committed CPU-restatement results of workload k (tests/golden), or None."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", f"cfg{k}.json")) as f:
+            return json.load(f)
+    except OSError:
+        return None
+
+
+POLAR = (("complex_polar", 1), ("receptor_polar", 4), ("ligand_polar", 7), ("delta_polar", 10))
+
+
+def _polar_err(a, b):
+    n = min(len(a), len(b))
+    return {k: float(np.abs(np.asarray(a)[:n, c] - np.asarray(b)[:n, c]).max()) for k, c in POLAR}
+
+
+def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs, rel_tols=(1e-6, 1e-7)):
+    """MM-PBSA on the 3,040-atom workload: frames/s of the batched engine on
+    the reference's stopping rule and on the relative-residual rule (FP32
+    V-cycles of a consistent multigrid under FP64 defect correction), beside
+    the plain FP64 form (reference schedule) on the first n_plain frames;
+    polar-term differences against the plain form and against the oracle's
+    golden rows (the reference's own iterate, and the converged solution)."""
     import torch
     S = _synthetic()
 
@@ -206,15 +226,17 @@ def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs):
     d = tempfile.mkdtemp()
     S.write_prmtop(s, os.path.join(d, "w3.prmtop"))
     top = rst.read_prmtop(os.path.join(d, "w3.prmtop"))
+    gold = _golden(3)
     out = {}
     for name, kw in (("linear_dh", PB), ("focusing_default", dict(fillratio=4.0))):
+        nf = n_frames if name == "linear_dh" else min(n_frames, 32)
         p = rst.PbParams(**kw)
         fused = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, pb_params=p, ctx=ctx)
-        fused.run(fr)  # warm-up at the timed size: the engine's pools are sized by the batch
+        fused.run(fr[:nf])  # warm-up at the timed size: the engine's pools are sized by the batch
         torch.cuda.synchronize()
         st0 = fused.pb_stats()
         t = time.perf_counter()
-        ef = fused.run(fr)
+        ef = fused.run(fr[:nf])
         tf = time.perf_counter() - t
         st = {k: v - st0[k] for k, v in fused.pb_stats().items()}  # the timed run alone
         plain = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, pb_params=p, mode="plain", ctx=ctx)
@@ -222,13 +244,32 @@ def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs):
         t = time.perf_counter()
         ep = plain.run(fr[:n_plain])
         tp = time.perf_counter() - t
-        keys = ("complex_polar", "receptor_polar", "ligand_polar", "delta_polar")
-        err = {k: float(np.abs(ef[:n_plain, c] - ep[:, c]).max()) for k, c in zip(keys, (1, 4, 7, 10))}
-        r = {"fused_frames_per_s": n_frames / tf, "plain_frames_per_s": n_plain / tp,
-             "speedup_vs_plain_gpu": (n_frames / tf) / (n_plain / tp), "frames": n_frames, "plain_frames": n_plain,
-             "max_abs_diff_vs_plain_fp64_kcal": err, "tolerance_kcal": 1e-3,
-             "grids": st["grids"], "lockstep_cycles": st["cycles"], "sor_grids": st["fp64_fallbacks"],
-             "host_ms_setup_cycles_finish": [st["ms_setup"], st["ms_cycles"], st["ms_finish"]]}
+        pv = n_plain / tp
+        r = {"reference_rule": {"fused_frames_per_s": nf / tf, "speedup_vs_plain_gpu": (nf / tf) / pv,
+                                "max_abs_diff_vs_plain_fp64_kcal": _polar_err(ef, ep),
+                                "grids": st["grids"], "lockstep_cycles": st["cycles"],
+                                "sor_grids": st["fp64_fallbacks"],
+                                "host_ms_setup_cycles_finish": [st["ms_setup"], st["ms_cycles"], st["ms_finish"]]},
+             "plain_frames_per_s": pv, "plain_frames": n_plain, "frames": nf, "tolerance_kcal": 1e-3}
+        if name == "linear_dh" and gold is not None:
+            r["reference_rule"]["max_abs_diff_vs_oracle_reference_iterate_kcal"] = _polar_err(ef, gold["pb_faithful"])
+            r["reference_rule"]["max_abs_diff_vs_oracle_converged_kcal"] = _polar_err(ef, gold["pb_converged"])
+            r["plain_max_abs_diff_vs_oracle_converged_kcal"] = _polar_err(ep, gold["pb_converged"])
+            r["oracle_frames"] = len(gold["pb_converged"])
+        for tol in rel_tols:
+            fused.set_pb_convergence(tol)
+            st0 = fused.pb_stats()
+            t = time.perf_counter()
+            er = fused.run(fr[:nf])
+            tr = time.perf_counter() - t
+            st = {k: v - st0[k] for k, v in fused.pb_stats().items()}
+            q = {"fused_frames_per_s": nf / tr, "speedup_vs_plain_gpu": (nf / tr) / pv,
+                 "lockstep_cycles": st["cycles"], "sor_grids": st["fp64_fallbacks"],
+                 "max_abs_diff_vs_plain_fp64_kcal": _polar_err(er, ep)}
+            if name == "linear_dh" and gold is not None:
+                q["max_abs_diff_vs_oracle_converged_kcal"] = _polar_err(er, gold["pb_converged"])
+            r[f"relative_residual_{tol:g}"] = q
+        fused.set_pb_convergence(0.0)
         if name == "linear_dh":  # HBM roofline of the level-0 kernels (event-timed, no graph capture)
             fused.set_pb_profile(True)
             fused.run(fr[:8])
@@ -411,7 +452,8 @@ def main():
     ap.add_argument("--ref-frames", type=int, default=8)
     ap.add_argument("--plain-frames", type=int, default=16)
     ap.add_argument("--serve-requests", type=int, default=48)
-    ap.add_argument("--pb-frames", type=int, default=32, help="MM-PBSA leg frames (0: skip)")
+    ap.add_argument("--pb-frames", type=int, default=100, help="MM-PBSA leg frames (0: skip)")
+    ap.add_argument("--pb-plain-frames", type=int, default=24, help="frames of the plain FP64 PB form")
     ap.add_argument("--no-large", action="store_true", help="skip the 25,080-atom mixed GB/PB serving leg")
     ap.add_argument("--pb-only", action="store_true", help="run only the MM-PBSA leg (--pb-frames frames) and print it")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e/plain/cpu/serving legs")
@@ -427,7 +469,7 @@ def main():
 
         torch.cuda.set_device(0)
         ctx = N.make_ctx(0, torch.cuda.current_stream().cuda_stream)
-        print(json.dumps(pbsa_leg(rst, ctx, args.pb_frames, args.pb_frames, hbm_peak())), flush=True)
+        print(json.dumps(pbsa_leg(rst, ctx, args.pb_frames, args.pb_plain_frames, hbm_peak())), flush=True)
         return
 
     import torch
@@ -564,7 +606,7 @@ def main():
             extras["serving"] = serving_stream(rst, ctx, args.serve_requests)
         if rank == 0 and world == 1 and args.pb_frames > 0:
             # plain on the same frames
-            extras["pbsa"] = pbsa_leg(rst, ctx, args.pb_frames, args.pb_frames, hbm_peak())
+            extras["pbsa"] = pbsa_leg(rst, ctx, args.pb_frames, args.pb_plain_frames, hbm_peak())
         if rank == 0 and world == 1 and not args.no_large:
             extras["large_mixed"] = large_mixed(rst, ctx)
 

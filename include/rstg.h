@@ -247,6 +247,15 @@ rstg_status rstg_decompose(rstg_ctx* ctx, const rstg_topology* t, const double* 
                            int64_t n_lig, const rstg_gb_params* gb, const rstg_sa_params* sa,
                            rstg_residue_energy* rec_out, rstg_residue_energy* lig_out);
 
+/* Mass-weighted coordinate covariance of quasi_harmonic_entropy,
+ * crates/mmpbsa/src/entropy.rs:97-160, in FP64 on the GPU: traj_A host
+ * [n_frames][n_atoms][3] Angstrom, masses [n_atoms] amu, cov host
+ * [3 n_atoms][3 n_atoms] (full symmetric, row-major), equal bit for bit to
+ * the reference's frame-ordered sums.  The eigenvalues and the entropy sum
+ * stay on the host. */
+rstg_status rstg_qh_covariance(rstg_ctx* ctx, const double* traj_A, int64_t n_frames, int64_t n_atoms,
+                               const double* masses, double* cov);
+
 /* GB energy (Born radii + pair sum, same kernels and results as
  * rstg_gb_energy_compute) that allocates no device memory.  No counterpart in
  * the reference.  For callers that cannot call cudaMalloc where they need the
@@ -273,9 +282,12 @@ typedef enum rstg_mode {
 typedef struct rstg_system_opts {
   int32_t mode;            /* rstg_mode, default FUSED                          */
   int32_t decompose;       /* also produce per-residue terms for every frame    */
-  int64_t max_batch_frames; /* frames per device batch (0: chosen by autotuner) */
+  int64_t max_batch_frames; /* frames per device batch (0: as many as fit a
+                              2 GB share of device memory, at most 256)      */
   int32_t use_graphs;      /* capture each batch's launch sequence (default 1) */
-  int32_t autotune;        /* time tile/launch shapes on first use (default 1) */
+  int32_t autotune;        /* time the launch shapes of the pair and SASA
+                              kernels on the first run and keep the fastest
+                              (default 1; 0: fixed default shapes)          */
 } rstg_system_opts;
 void rstg_system_opts_default(rstg_system_opts* o);
 
@@ -307,6 +319,17 @@ rstg_status rstg_system_run_device(rstg_system* s, const float* d_frames, int64_
  * [0] launches, [1] pairs sent to the FP64 guard path, [2] SASA point tests
  * re-checked in FP64, [3] neighbour-list overflows (must be 0). */
 rstg_status rstg_system_last_stats(const rstg_system* s, int64_t* stats4);
+
+/* Launch shapes of a fused system (no reference counterpart).  shape8 =
+ * pair-kernel threads per tile row, its minimum resident blocks per SM
+ * (register cap), SASA warps per block, frames per batch, tuned (1 once the
+ * first run timed the candidates), frames of the tuning pass, number of
+ * pair-kernel candidates, number of SASA candidates; ms8 = the tuning pass's
+ * best-of-two milliseconds per candidate (pair-kernel shapes first, then
+ * SASA shapes).  Systems of one process with the same device, atom counts
+ * and sphere points share the tuned shapes, so equal inputs give equal
+ * results.  Either pointer may be NULL; zeros for plain-mode systems. */
+rstg_status rstg_system_tuning(const rstg_system* s, int32_t* shape8, double* ms8);
 
 /* Batched Poisson-Boltzmann engine of a fused PB system (no reference
  * counterpart), accumulated over runs: grids solved, lock-step multigrid

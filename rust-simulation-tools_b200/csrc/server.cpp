@@ -54,6 +54,7 @@ struct Server {
   int64_t resident_total = 0, peak_bytes = 0, next_id = 1, frames_done = 0;
   int running = 0;
   bool stop = false;
+  int64_t device_bytes = 0;  // a request whose buffers exceed the device is refused at submit
   std::vector<double> latencies_ms;
   Clock::time_point first_submit, last_done;
   bool any = false;
@@ -61,6 +62,9 @@ struct Server {
   Server(Ctx* c, const rstg_server_opts& o) : ctx(c), opts(o) {
     int n = std::max(1, opts.max_inflight);
     c->bind();
+    size_t fr = 0, tot = 0;
+    RSTG_CUDA(cudaMemGetInfo(&fr, &tot));
+    device_bytes = (int64_t)tot;
     streams = take_streams(c->device, n);
     for (int k = 0; k < n; k++) slots.emplace_back([this, k] { slot_loop(k); });
   }
@@ -224,6 +228,9 @@ struct Server {
     r->frames.assign(frames, frames + (size_t)F * sys->n_top * 3);
     r->out.resize(F);
     r->bytes = sys->footprint(std::min<int64_t>(F, sys->batch > 0 ? sys->batch : F));
+    if (r->bytes > device_bytes)
+      throw Error(RSTG_ERR_NOMEM, "request needs " + std::to_string(r->bytes) + " bytes of device memory; the device has " +
+                                      std::to_string(device_bytes));
     std::lock_guard<std::mutex> lk(mu);
     r->id = next_id++;
     r->submitted = Clock::now();
@@ -244,7 +251,10 @@ struct Server {
   }
 
   rstg_status collect(const std::shared_ptr<Request>& r, rstg_frame_energy* out) {
-    if (r->state == Request::CANCELLED) return RSTG_ERR_CANCELLED;
+    if (r->state == Request::CANCELLED) {
+      set_last_error("request " + std::to_string(r->id) + " was cancelled");
+      return RSTG_ERR_CANCELLED;
+    }
     if (r->state == Request::FAILED) {
       set_last_error(r->msg);
       return r->err;

@@ -32,7 +32,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <tuple>
 #include <unordered_map>
 
 #include "common.cuh"
@@ -45,12 +48,12 @@ namespace rstg {
 // redone in FP64 with the reference's rounding
 static constexpr float kSasaBand = 2e-4f;
 static constexpr float kNbGuard2 = 3.5f * 3.5f;
-static constexpr int kSasaWarps = 4;
 
-static size_t sasa_smem(int cap) {
+// shared memory of a k_sasa block of `warps` warps
+static size_t sasa_smem(int cap, int warps) {
   size_t cap2 = 32;
   while ((int)cap2 < cap) cap2 <<= 1;
-  return (size_t)kSasaWarps * (cap * sizeof(float4) + cap2 * (sizeof(float) + sizeof(int)));
+  return (size_t)warps * (cap * sizeof(float4) + cap2 * (sizeof(float) + sizeof(int)));
 }
 
 struct GbConstF {
@@ -343,13 +346,23 @@ struct PairOut {
   double gbC, gbR, gbL, dgb, mmR, mmL;
 };
 
-__global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __restrict__ tiles,
-                                                 const float4* __restrict__ xyz32, const double* __restrict__ xyz64,
-                                                 const float4* __restrict__ Rf, const float* __restrict__ dRf,
-                                                 const int* __restrict__ type, int nt,
-                                                 const float2* __restrict__ lj32, const double2* __restrict__ lj64,
-                                                 const unsigned* __restrict__ masks, GbConstF k, double scee,
-                                                 double scnb, double* __restrict__ part, int* __restrict__ diag) {
+// One 128 x 128 tile per block.  TPR threads share a row: thread
+// (row, part) takes the row's columns [part*128/TPR, (part+1)*128/TPR), so
+// TPR > 1 gives more, smaller threads per tile (TPR and the register cap
+// MINB are picked per system by the tuner).  Pairs whose Lennard-Jones /
+// Coulomb term takes the FP64 path (closer than 3.5 A, or 1-4) are marked in
+// a per-thread bit mask and evaluated after the column loop, each thread over
+// its own marks, so a warp runs as many FP64 evaluations as its busiest lane
+// rather than one for every column where any lane needs one.
+template <int TPR, int MINB>
+__global__ void __launch_bounds__(kTile * TPR, MINB)
+    k_pairs(int nC, int nR, const int4* __restrict__ tiles, const float4* __restrict__ xyz32,
+            const double* __restrict__ xyz64, const float4* __restrict__ Rf, const float* __restrict__ dRf,
+            const int* __restrict__ type, int nt, const float2* __restrict__ lj32, const double2* __restrict__ lj64,
+            const unsigned* __restrict__ masks, GbConstF k, double scee, double scnb, double* __restrict__ part,
+            int* __restrict__ diag) {
+  constexpr int kCols = kTile / TPR, kWords = kCols / 32;
+  static_assert(kCols % 32 == 0, "columns per thread in whole words");
   extern __shared__ float2 slj[];  // nt*nt (A, B)
   __shared__ float4 sx[kTile];
   __shared__ float4 sR[kTile];
@@ -359,17 +372,20 @@ __global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __r
   for (int t = threadIdx.x; t < nt * nt; t += blockDim.x) slj[t] = lj32[t];
   int4 tl = tiles[blockIdx.x];
   int f = blockIdx.y, bi = tl.x, bj = tl.y, rec = tl.z;
-  int i = bi * kTile + threadIdx.x, j0 = bj * kTile;
+  const int row = threadIdx.x % kTile, cpart = threadIdx.x / kTile;
+  int i = bi * kTile + row, j0 = bj * kTile;
   const float4* X = xyz32 + (long long)f * nC;
   const double* X64 = xyz64 + (long long)f * nC * 3;
   const float4* RF = Rf + (long long)f * nC;
   const float* DR = dRf + (long long)f * nC;
-  int jl = j0 + threadIdx.x;
-  if (jl < nC) {
-    sx[threadIdx.x] = X[jl];
-    sR[threadIdx.x] = RF[jl];
-    sdR[threadIdx.x] = DR[jl];
-    st[threadIdx.x] = type[jl];
+  if (threadIdx.x < kTile) {
+    int jl = j0 + threadIdx.x;
+    if (jl < nC) {
+      sx[threadIdx.x] = X[jl];
+      sR[threadIdx.x] = RF[jl];
+      sdR[threadIdx.x] = DR[jl];
+      st[threadIdx.x] = type[jl];
+    }
   }
   __syncthreads();
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -381,20 +397,29 @@ __global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __r
     int ti = type[i];
     bool in_r = i < nR;
     float iRc = Ri.z, iRs = Ri.w;
-    unsigned mex[4] = {0, 0, 0, 0}, m14[4] = {0, 0, 0, 0};
+    const int cb = cpart * kCols;  // first column of this thread
+    unsigned mex[kWords], m14[kWords], defer[kWords];
+#pragma unroll
+    for (int w = 0; w < kWords; w++) mex[w] = m14[w] = defer[w] = 0u;
     if (rec >= 0) {
-      const unsigned* mr = masks + ((long long)rec * 2 * kTile + threadIdx.x) * 4;
-      for (int w = 0; w < 4; w++) {
+      const unsigned* mr = masks + ((long long)rec * 2 * kTile + row) * 4 + cb / 32;
+#pragma unroll
+      for (int w = 0; w < kWords; w++) {
         mex[w] = mr[w];
         m14[w] = mr[kTile * 4 + w];
       }
     }
-    int m = min(kTile, nC - j0);
-    int jstart = (bi == bj) ? threadIdx.x + 1 : 0;
-    for (int c0 = jstart; c0 < m; c0 += 32) {
+    int m = min(cb + kCols, nC - j0);
+    int jstart = (bi == bj) ? max(row + 1, cb) : cb;
+    // one 32-column word of the masks per step (unrolled: the mask words stay in registers)
+#pragma unroll
+    for (int w = 0; w < kWords; w++) {
+      const int lo = max(cb + 32 * w, jstart), hi = min(cb + 32 * w + 32, m);
+      if (lo >= hi) continue;
+      const unsigned wex = mex[w], w14 = m14[w];
+      unsigned dfr = 0u;
       float a[6] = {0, 0, 0, 0, 0, 0};
-      int cend = min(m, c0 + 32);
-      for (int jj = c0; jj < cend; jj++) {
+      for (int jj = lo; jj < hi; jj++) {
         int j = j0 + jj;
         float4 xj = sx[jj];
         float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
@@ -419,31 +444,37 @@ __global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __r
                          : gb_pair_delta(qq, r2, RRc, Ri.y * Rj.y, iRRs, dRR, tc, ts, eC, f2C, finvC, EC, k);
           a[in_r ? 1 : 2] += pC - dp;
           a[3] += dp;
-          int cls = 1;
-          if (rec >= 0) {
-            int w = jj >> 5, b = jj & 31;
-            if ((m14[w] >> b) & 1u)
-              cls = 2;
-            else if ((mex[w] >> b) & 1u)
-              cls = 0;
-          }
-          if (cls) {
-            int tj = st[jj];
-            if (r2 < kNbGuard2 || cls == 2) {
-              double2 ab = lj64[ti * nt + tj];
-              double e = nb64(X64, i, j, (double)qq, ab.x, ab.y, cls, scee, scnb);
-              acc[in_r ? 4 : 5] += e;
-              n64++;
-            } else {
-              float2 ab = slj[ti * nt + tj];
-              float rinv = rsqrtf(r2), ir2 = rinv * rinv, ir6 = ir2 * ir2 * ir2;
-              a[in_r ? 4 : 5] += fmaf(ab.x * ir6, ir6, fmaf(-ab.y, ir6, qq * rinv));
-            }
+          const int b = jj & 31;
+          const bool is14 = (w14 >> b) & 1u, excl = (wex >> b) & 1u;
+          if (is14 || (!excl && r2 < kNbGuard2)) {
+            dfr |= 1u << b;
+          } else if (!excl) {
+            float2 ab = slj[ti * nt + st[jj]];
+            float rinv = rsqrtf(r2), ir2 = rinv * rinv, ir6 = ir2 * ir2 * ir2;
+            a[in_r ? 4 : 5] += fmaf(ab.x * ir6, ir6, fmaf(-ab.y, ir6, qq * rinv));
           }
         }  // receptor x ligand GB pairs enter the binding difference in FP64 (k_rl_rows)
       }
+      defer[w] = dfr;
+#pragma unroll
       for (int q = 0; q < 6; q++) acc[q] += (double)a[q];
     }
+    // deferred FP64 Lennard-Jones / Coulomb pairs of this thread
+    double e64 = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWords; w++) {
+      unsigned mk = defer[w];
+      while (mk) {
+        const int b = __ffs(mk) - 1;
+        mk &= mk - 1;
+        const int jj = cb + 32 * w + b, j = j0 + jj;
+        const int cls = ((m14[w] >> b) & 1u) ? 2 : 1;
+        const double2 ab = lj64[ti * nt + st[jj]];
+        e64 += nb64(X64, i, j, (double)xi.w * (double)sx[jj].w, ab.x, ab.y, cls, scee, scnb);
+        n64++;
+      }
+    }
+    acc[in_r ? 4 : 5] += e64;
   }
   if (n64) atomicAdd((unsigned long long*)(diag + 4), (unsigned long long)n64);
   double* p = part + ((long long)f * gridDim.x + blockIdx.x) * 6;
@@ -452,6 +483,21 @@ __global__ void __launch_bounds__(kTile) k_pairs(int nC, int nR, const int4* __r
     if (threadIdx.x == 0) p[q] = v;
   }
 }
+
+// Launch shapes of k_pairs the tuner chooses from: threads per row (TPR) and
+// the minimum resident blocks per SM that caps registers per thread.
+using PairsFn = void (*)(int, int, const int4*, const float4*, const double*, const float4*, const float*,
+                         const int*, int, const float2*, const double2*, const unsigned*, GbConstF, double, double,
+                         double*, int*);
+struct PairsVariant {
+  int tpr, minb;
+  PairsFn fn;
+};
+static const PairsVariant kPairsVariants[] = {
+    {1, 6, k_pairs<1, 6>}, {1, 4, k_pairs<1, 4>}, {2, 3, k_pairs<2, 3>}, {2, 4, k_pairs<2, 4>}, {4, 2, k_pairs<4, 2>}};
+constexpr int kNumPairsVariants = (int)(sizeof(kPairsVariants) / sizeof(kPairsVariants[0]));
+static const int kSasaWarpChoices[] = {4, 2, 8};
+constexpr int kNumSasaChoices = 3;
 
 // ---------------------------------------------------------------------------
 // K3: SASA (one warp per atom), own-part then other-part neighbours
@@ -1040,7 +1086,8 @@ void System::prepare_fused(const double* x0) {
   up(F.tiles, tiles.data(), tiles.size() * sizeof(int4));
   size_t ljsm = (size_t)nt * nt * sizeof(float2);
   if (ljsm > 160 * 1024) throw Error(RSTG_ERR_INVALID, "too many Lennard-Jones types for the fused kernels");
-  RSTG_CUDA(cudaFuncSetAttribute(k_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ljsm));
+  for (const PairsVariant& v : kPairsVariants)
+    RSTG_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ljsm));
   up(F.tile_rec, trec.data(), trec.size() * 4);
   up(F.masks, masks.data(), masks.size() * 4);
   // sphere points (host libm, as the reference)
@@ -1201,14 +1248,125 @@ void System::ensure_buffers(int64_t frames) {
   dec_buf = DevBuf(B * std::max<int64_t>(fp->nres, 1) * sizeof(rstg_residue_energy), st);
   diag = DevBuf(64, st);
   RSTG_CUDA(cudaMemsetAsync(diag.p, 0, 64, st));
-  size_t sm = sasa_smem(nbr_cap);
-  if (sm > 200 * 1024) throw Error(RSTG_ERR_INVALID, "SASA neighbour capacity exceeds shared memory");
+  if (sasa_smem(nbr_cap, 2) > 200 * 1024) throw Error(RSTG_ERR_INVALID, "SASA neighbour capacity exceeds shared memory");
+  while (sasa_smem(nbr_cap, sasa_warps) > 200 * 1024) sasa_warps /= 2;  // a capacity grown on overflow
+  size_t sm = 0;
+  for (int w : kSasaWarpChoices)
+    if (sasa_smem(nbr_cap, w) <= 200 * 1024) sm = std::max(sm, sasa_smem(nbr_cap, w));
   RSTG_CUDA(cudaFuncSetAttribute(k_sasa, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   buf_frames = B;
   if (graph) {
     cudaGraphExecDestroy(graph);
     graph = nullptr;
   }
+}
+
+void System::launch_pairs(int variant, int64_t F) {
+  FusedParams& P = *fp;
+  const PairsVariant& v = kPairsVariants[variant];
+  size_t ljsm = (size_t)P.nt * P.nt * sizeof(float2);
+  v.fn<<<dim3((unsigned)P.ntiles, (unsigned)F), kTile * v.tpr, ljsm, stream()>>>(
+      (int)nC, (int)nR, P.tiles.as<int4>(), xyz32.as<float4>(), xyz64.as<double>(), Rf.as<float4>(), dRf.as<float>(),
+      P.type.as<int>(), P.nt, P.lj32.as<float2>(), P.lj64.as<double2>(), P.masks.as<unsigned>(), P.gb,
+      split.complex.scee, split.complex.scnb, k2part.as<double>(), diag.as<int>());
+}
+
+void System::launch_sasa(int warps, int64_t F) {
+  FusedParams& P = *fp;
+  size_t sm = sasa_smem(nbr_cap, warps);
+  k_sasa<<<dim3((unsigned)((nC + warps - 1) / warps), (unsigned)F), 32 * warps, sm, stream()>>>(
+      (int)nC, (int)nR, nbr_cap, nbr.as<int>(), nbrcnt.as<int>(), xyz32.as<float4>(), xyz64.as<double>(),
+      P.rad64.as<double>(), P.probe, P.npts, P.sphere32.as<float4>(), P.sphere64.as<double>(), sasa.as<double>(),
+      diag.as<int>());
+}
+
+// Kernel shapes per system shape, shared by every system of this process
+// with the same device and sizes, so equal inputs give equal bits.
+struct TuneKey {
+  int device;
+  int64_t nC, nR, npts;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(device, nC, nR, npts) < std::tie(o.device, o.nC, o.nR, o.npts);
+  }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, std::pair<int, int>> g_tuned;
+
+// Times every launch shape of k_pairs and k_sasa on the first frames of the
+// first run (inputs already in in_frames; one warm pass fills the buffers
+// they read) and keeps the fastest of each: best of two CUDA-event timed
+// launches on the system stream.
+void System::tune(bool f64, int64_t B) {
+  TuneKey key{ctx->device, nC, nR, fp->npts};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      pairs_variant = it->second.first;
+      sasa_warps = it->second.second;
+      tuned = true;
+      return;
+    }
+  }
+  cudaStream_t st = stream();
+  int64_t TB = std::min<int64_t>(B, 64);
+  launch_batch(in_frames.p, f64, TB, res_buf.as<rstg_frame_energy>(), nullptr);
+  cudaEvent_t a, b;
+  RSTG_CUDA(cudaEventCreate(&a));
+  RSTG_CUDA(cudaEventCreate(&b));
+  auto time_it = [&](auto&& launch) {
+    float best = 1e30f;
+    for (int rep = 0; rep < 2; rep++) {
+      RSTG_CUDA(cudaEventRecord(a, st));
+      launch();
+      RSTG_CUDA(cudaEventRecord(b, st));
+      RSTG_CUDA(cudaEventSynchronize(b));
+      float t = 0.f;
+      RSTG_CUDA(cudaEventElapsedTime(&t, a, b));
+      best = std::min(best, t);
+    }
+    launched(ctx, 2);
+    return best;
+  };
+  try {
+    float bp = 1e30f;
+    for (int v = 0; v < kNumPairsVariants; v++) {
+      tune_ms[v] = time_it([&] { launch_pairs(v, TB); });
+      if (tune_ms[v] < bp) {
+        bp = (float)tune_ms[v];
+        pairs_variant = v;
+      }
+    }
+    float bs = 1e30f;
+    for (int c = 0; c < kNumSasaChoices; c++) {
+      int w = kSasaWarpChoices[c];
+      double t = sasa_smem(nbr_cap, w) <= 200 * 1024 ? time_it([&] { launch_sasa(w, TB); }) : 1e30;
+      tune_ms[kNumPairsVariants + c] = t;
+      if (t < bs) {
+        bs = (float)t;
+        sasa_warps = w;
+      }
+    }
+  } catch (...) {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    throw;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  tune_frames = TB;
+  tuned = true;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned.emplace(key, std::make_pair(pairs_variant, sasa_warps));
+}
+
+void System::tuning(int32_t* shape8, double* ms8) const {
+  const PairsVariant& v = kPairsVariants[pairs_variant];
+  int32_t o[8] = {v.tpr, v.minb, sasa_warps, (int32_t)batch, tuned ? 1 : 0, (int32_t)tune_frames,
+                  kNumPairsVariants, kNumSasaChoices};
+  if (shape8) memcpy(shape8, o, sizeof(o));
+  if (ms8)
+    for (int k = 0; k < 8; k++) ms8[k] = tune_ms[k];
 }
 
 void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_energy* d_out,
@@ -1245,18 +1403,9 @@ void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_
                                                    R64.as<double>(), Rf.as<float4>(), dRf.as<float>(), k1part.as<double>(),
                                                    diag.as<int>());
   mark("psi", Fd * nCd * (nCd - 1) * 32.0, 0.0);
-  size_t ljsm = (size_t)P.nt * P.nt * sizeof(float2);
-  k_pairs<<<dim3((unsigned)P.ntiles, Fu), kTile, ljsm, st>>>(
-      (int)nC, (int)nR, P.tiles.as<int4>(), xyz32.as<float4>(), xyz64.as<double>(), Rf.as<float4>(), dRf.as<float>(),
-      P.type.as<int>(),
-      P.nt, P.lj32.as<float2>(), P.lj64.as<double2>(), P.masks.as<unsigned>(), P.gb, split.complex.scee,
-      split.complex.scnb, k2part.as<double>(), diag.as<int>());
+  launch_pairs(pairs_variant, F);
   mark("pairs", Fd * (nCd * (nCd - 1) / 2 * gbf + same_pairs * (gbf + 22.0)), 0.0);
-  size_t sm = sasa_smem(nbr_cap);
-  k_sasa<<<dim3((unsigned)((nC + kSasaWarps - 1) / kSasaWarps), Fu), 32 * kSasaWarps, sm, st>>>(
-      (int)nC, (int)nR, nbr_cap, nbr.as<int>(), nbrcnt.as<int>(), xyz32.as<float4>(), xyz64.as<double>(),
-      P.rad64.as<double>(), P.probe, P.npts, P.sphere32.as<float4>(), P.sphere64.as<double>(), sasa.as<double>(),
-      diag.as<int>());
+  launch_sasa(sasa_warps, F);
   mark("sasa", 0.0, 0.0);
   int nlaunch = 4;
   if (nR > 0 && nL > 0) {
@@ -1503,6 +1652,12 @@ void System::run(const void* frames, bool f64, bool host_in, int64_t F, rstg_fra
   int64_t nres = fp->nres;
   for (int attempt = 0; attempt < 3; attempt++) {
     ensure_buffers(std::min(F, batch));
+    if (!tuned && opts.autotune) {
+      int64_t B = std::min(batch, F);
+      RSTG_CUDA(cudaMemcpyAsync(in_frames.p, frames, (size_t)B * n_top * 3 * esz,
+                                host_in ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+      tune(f64, B);
+    }
     RSTG_CUDA(cudaMemsetAsync(diag.p, 0, 64, st));
     last_stats[0] = 0;
     for (int64_t f0 = 0; f0 < F; f0 += batch) {

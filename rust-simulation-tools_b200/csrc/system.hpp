@@ -34,6 +34,13 @@ struct System {
   std::unique_ptr<FusedParams> fp;
   int64_t batch = 0;  // frames per device batch
   int nbr_cap = 320;
+  // launch shapes (picked by tune() on the first run when opts.autotune)
+  int pairs_variant = 0;  // index into the k_pairs shape table (system.cu)
+  int sasa_warps = 4;     // warps (atoms) per k_sasa block
+  bool tuned = false;
+  int64_t tune_frames = 0;
+  double tune_ms[8] = {};  // candidate times of the tuning run (k_pairs shapes, then k_sasa shapes)
+  void tuning(int32_t* shape8, double* ms8) const;
 
   // per-batch buffers (fused)
   DevBuf in_frames, xyz64, xyz32, R64, Rf, dRf, nbr, nbrcnt, sasa, k1part, k2part, rows, cols, bpart, res_buf, dec_buf,
@@ -76,6 +83,9 @@ struct System {
   };
   void launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_energy* d_out,
                     rstg_residue_energy* d_decomp, Prof* prof = nullptr);
+  void launch_pairs(int variant, int64_t F);
+  void launch_sasa(int warps, int64_t F);
+  void tune(bool f64, int64_t B);
 
  public:
   void profile(const float* d_frames, int64_t F, int32_t* n, char* names, double* ms, double* flops, double* bytes);

@@ -84,7 +84,10 @@ DcdData read_dcd(const std::string& path) {
       double c6[6];
       memcpy(c6, &buf[pos + 4], 48);
       pos += 56;
-      d.boxes.push_back({c6[0], c6[2], c6[5]});  // a, b, c in Angstrom
+      // a, b, c (CHARMM order a, gamma, b, beta, alpha, c); the reference
+      // stores them in nm (dcd.rs:383-400) and scales by 10 for reimaging
+      // (binding.rs:635-642): the same roundings here
+      d.boxes.push_back({(c6[0] * 0.1) * 10.0, (c6[2] * 0.1) * 10.0, (c6[5] * 0.1) * 10.0});
     }
     for (int dim = 0; dim < 3; dim++) {
       i32();

@@ -707,7 +707,7 @@ class BindingSystem:
 
     def __init__(self, topology: AmberTopology, receptor_residues, ligand_residues, gb_params: GbParams = None,
                  pb_params: PbParams = None, sa_params: SaParams = None, mode: str = "fused",
-                 batch_frames: int = 0, use_graphs: bool = True, ctx=None):
+                 batch_frames: int = 0, use_graphs: bool = True, autotune: bool = True, ctx=None):
         self.topology = topology
         self.ctx = ctx or N.ctx()
         rr, lr = _i64(receptor_residues), _i64(ligand_residues)
@@ -716,6 +716,7 @@ class BindingSystem:
         o.mode = 0 if mode == "plain" else 1
         o.max_batch_frames = int(batch_frames)
         o.use_graphs = int(use_graphs)
+        o.autotune = int(autotune)
         h = N.vp()
         check(N.lib.rstg_system_create(self.ctx, topology._h, _ip(rr), len(rr), _ip(lr), len(lr),
                                        C.byref(_solvation(gb_params, pb_params)), C.byref(_sa(sa_params)),
@@ -766,6 +767,17 @@ class BindingSystem:
         check(N.lib.rstg_system_last_stats(self._h, _ip(st)))
         return {"launches": int(st[0]), "fp64_guard_pairs": int(st[1]), "sasa_rechecks": int(st[2]),
                 "neighbour_overflow": int(st[3])}
+
+    def tuning(self) -> dict:
+        """Launch shapes of the fused engine (picked on the first run when
+        autotuning) and the tuning pass's candidate times in ms."""
+        sh = (C.c_int32 * 8)()
+        ms = np.zeros(8)
+        check(N.lib.rstg_system_tuning(self._h, sh, _dp(ms)))
+        npair, nsasa = sh[6], sh[7]
+        return {"pairs_threads_per_row": sh[0], "pairs_min_blocks_per_sm": sh[1], "sasa_warps_per_block": sh[2],
+                "batch_frames": sh[3], "tuned": bool(sh[4]), "tuning_frames": sh[5],
+                "pairs_candidates_ms": ms[:npair].tolist(), "sasa_candidates_ms": ms[npair:npair + nsasa].tolist()}
 
     def pb_stats(self) -> dict:
         """Batched PB engine totals of a fused PB system (zeros otherwise)."""

@@ -134,6 +134,7 @@ _sig("rstg_binding_frame", C.c_int, vp, vp, dp, i64, ip, i64, ip, i64, P(Solvati
 _sig("rstg_decompose", C.c_int, vp, vp, dp, i64, ip, i64, ip, i64, P(GbParams), P(SaParams), P(ResidueEnergy),
      P(ResidueEnergy))
 _sig("rstg_gb_energy_noalloc_async", C.c_int, vp, vp, vp, vp, i64, P(GbParams), vp, vp, vp)
+_sig("rstg_qh_covariance", C.c_int, vp, dp, i64, i64, dp, dp)
 _sig("rstg_system_opts_default", None, P(SystemOpts))
 _sig("rstg_system_create", C.c_int, vp, vp, ip, i64, ip, i64, P(Solvation), P(SaParams), P(SystemOpts), P(vp))
 _sig("rstg_system_destroy", None, vp)
@@ -143,6 +144,7 @@ _sig("rstg_system_run", C.c_int, vp, fp, i64, P(FrameEnergy), P(ResidueEnergy))
 _sig("rstg_system_run_device", C.c_int, vp, vp, i64, vp, vp)
 _sig("rstg_system_last_stats", C.c_int, vp, ip)
 _sig("rstg_system_pb_stats", C.c_int, vp, dp)
+_sig("rstg_system_tuning", C.c_int, vp, P(i32), dp)
 _sig("rstg_system_set_pb_batch", C.c_int, vp, i64)
 _sig("rstg_system_set_pb_profile", C.c_int, vp, i32)
 _sig("rstg_system_set_pb_convergence", C.c_int, vp, dbl)
@@ -165,6 +167,10 @@ class CudaError(RuntimeError):
     pass
 
 
+class RequestCancelled(RuntimeError):
+    """A serving request was cancelled before its results were delivered."""
+
+
 def check(rc: int) -> None:
     """Raise the Python exception the reference raises for this failure."""
     if rc == OK:
@@ -178,6 +184,8 @@ def check(rc: int) -> None:
         raise MemoryError(msg)
     if rc == ERR_TIMEOUT:
         raise TimeoutError(msg)
+    if rc == ERR_CANCELLED:
+        raise RequestCancelled(msg)
     raise ValueError(msg)
 
 

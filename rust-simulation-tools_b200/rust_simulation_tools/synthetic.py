@@ -143,14 +143,22 @@ def _fmt(values, per_line, fmt):
     return lines if lines else [""]
 
 
-def write_prmtop(system: System, path: str) -> None:
+def write_prmtop(system: System, path: str, bonds=None) -> None:
+    """AMBER prmtop of the system.  bonds: optional (i, j) atom pairs written
+    as BONDS_WITHOUT_HYDROGEN with one bond type of zero force constant (they
+    add no energy and no exclusion; they make molecules connected for
+    periodic reimaging)."""
     n = system.n_atoms
+    bonds = [] if bonds is None else [(int(i), int(j)) for i, j in bonds]
     nres = len(system.residue_labels)
     ntypes = len(system.sigma)
     a, b, nbi = lj_tables(system)
     pointers = [0] * 31
     pointers[0], pointers[1], pointers[11] = n, ntypes, nres
     pointers[10] = n  # NNB: one placeholder exclusion per atom
+    if bonds:
+        pointers[3] = pointers[12] = len(bonds)  # MBONA, NBONA
+        pointers[15] = 1  # NUMBND
     out = ["%VERSION  VERSION_STAMP = V0001.000  synthetic", "%FLAG TITLE", "%FORMAT(20a4)", "synthetic"]
 
     def sec(flag, fmt_name, lines):
@@ -170,15 +178,20 @@ def write_prmtop(system: System, path: str) -> None:
     labels = [lab.ljust(4)[:4] for lab in system.residue_labels]
     sec("RESIDUE_LABEL", "20a4", ["".join(labels[s:s + 20]) for s in range(0, nres, 20)])
     sec("RESIDUE_POINTER", "10I8", _fmt(list(system.residue_pointers[:nres] + 1), 10, "%8d"))
-    for flag in ("BOND_FORCE_CONSTANT", "BOND_EQUIL_VALUE", "ANGLE_FORCE_CONSTANT", "ANGLE_EQUIL_VALUE",
+    sec("BOND_FORCE_CONSTANT", "5E16.8", _fmt([0.0], 5, "%16.8E") if bonds else [""])
+    sec("BOND_EQUIL_VALUE", "5E16.8", _fmt([1.0], 5, "%16.8E") if bonds else [""])
+    for flag in ("ANGLE_FORCE_CONSTANT", "ANGLE_EQUIL_VALUE",
                  "DIHEDRAL_FORCE_CONSTANT", "DIHEDRAL_PERIODICITY", "DIHEDRAL_PHASE"):
         sec(flag, "5E16.8", [""])
     sec("SCEE_SCALE_FACTOR", "5E16.8", [""])
     sec("SCNB_SCALE_FACTOR", "5E16.8", [""])
     sec("LENNARD_JONES_ACOEF", "5E16.8", _fmt(list(a), 5, "%16.8E"))
     sec("LENNARD_JONES_BCOEF", "5E16.8", _fmt(list(b), 5, "%16.8E"))
-    for flag in ("BONDS_INC_HYDROGEN", "BONDS_WITHOUT_HYDROGEN", "ANGLES_INC_HYDROGEN", "ANGLES_WITHOUT_HYDROGEN",
-                 "DIHEDRALS_INC_HYDROGEN", "DIHEDRALS_WITHOUT_HYDROGEN"):
+    sec("BONDS_INC_HYDROGEN", "10I8", [""])
+    sec("BONDS_WITHOUT_HYDROGEN", "10I8",
+        _fmt([v for i, j in bonds for v in (3 * i, 3 * j, 1)], 10, "%8d") if bonds else [""])
+    for flag in ("ANGLES_INC_HYDROGEN", "ANGLES_WITHOUT_HYDROGEN", "DIHEDRALS_INC_HYDROGEN",
+                 "DIHEDRALS_WITHOUT_HYDROGEN"):
         sec(flag, "10I8", [""])
     sec("EXCLUDED_ATOMS_LIST", "10I8", _fmt([0] * n, 10, "%8d"))
     sec("RADIUS_SET", "1a80", ["modified Bondi radii (mbondi2)"])
@@ -188,13 +201,15 @@ def write_prmtop(system: System, path: str) -> None:
         f.write("\n".join(out) + "\n")
 
 
-def write_dcd(frames_A: np.ndarray, path: str) -> None:
-    """CHARMM-layout little-endian DCD without a unit cell (float32 Angstrom)."""
+def write_dcd(frames_A: np.ndarray, path: str, cell=None) -> None:
+    """CHARMM-layout little-endian DCD (float32 Angstrom).  cell: optional
+    (a, b, c, alpha, beta, gamma) in Angstrom and degrees, written before
+    every frame in CHARMM order (a, gamma, b, beta, alpha, c)."""
     frames_A = np.ascontiguousarray(frames_A, dtype=np.float32)
     nf, na, _ = frames_A.shape
     with open(path, "wb") as f:
         icntrl = [nf, 0, 1, nf, 0, 0, 0, 0, 0]
-        hdr = b"CORD" + struct.pack("<9i", *icntrl) + struct.pack("<f", 1.0) + struct.pack("<i", 0)
+        hdr = b"CORD" + struct.pack("<9i", *icntrl) + struct.pack("<f", 1.0) + struct.pack("<i", 1 if cell else 0)
         hdr += b"\x00" * 32 + struct.pack("<i", 24)
         f.write(struct.pack("<i", len(hdr)) + hdr + struct.pack("<i", len(hdr)))
         title = b"synthetic MM-GBSA workload".ljust(80)
@@ -203,6 +218,9 @@ def write_dcd(frames_A: np.ndarray, path: str) -> None:
         f.write(struct.pack("<iii", 4, na, 4))
         nb = struct.pack("<i", 4 * na)
         for fr in range(nf):
+            if cell:
+                a, b, c, al, be, ga = (float(v) for v in cell)
+                f.write(struct.pack("<i", 48) + struct.pack("<6d", a, ga, b, be, al, c) + struct.pack("<i", 48))
             for d in range(3):
                 f.write(nb + frames_A[fr, :, d].tobytes() + nb)
 
