@@ -263,11 +263,19 @@ def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs, rel_tols=(1e-6, 1e-7)):
             er = fused.run(fr[:nf])
             tr = time.perf_counter() - t
             st = {k: v - st0[k] for k, v in fused.pb_stats().items()}
-            q = {"fused_frames_per_s": nf / tr, "speedup_vs_plain_gpu": (nf / tr) / pv,
+            plain.set_pb_convergence(tol)  # the plain FP64 form on the same rule
+            t = time.perf_counter()
+            epr = plain.run(fr[:n_plain])
+            tpr = time.perf_counter() - t
+            plain.set_pb_convergence(0.0)
+            q = {"fused_frames_per_s": nf / tr, "speedup_vs_plain_gpu_reference_rule": (nf / tr) / pv,
+                 "plain_frames_per_s_same_rule": n_plain / tpr,
+                 "speedup_vs_plain_gpu_same_rule": (nf / tr) / (n_plain / tpr),
                  "lockstep_cycles": st["cycles"], "sor_grids": st["fp64_fallbacks"],
-                 "max_abs_diff_vs_plain_fp64_kcal": _polar_err(er, ep)}
+                 "max_abs_diff_vs_plain_fp64_same_rule_kcal": _polar_err(er, epr)}
             if name == "linear_dh" and gold is not None:
                 q["max_abs_diff_vs_oracle_converged_kcal"] = _polar_err(er, gold["pb_converged"])
+                q["plain_max_abs_diff_vs_oracle_converged_kcal"] = _polar_err(epr, gold["pb_converged"])
             r[f"relative_residual_{tol:g}"] = q
         fused.set_pb_convergence(0.0)
         if name == "linear_dh":  # HBM roofline of the level-0 kernels (event-timed, no graph capture)
@@ -317,18 +325,21 @@ def _fifo_latencies(arrivals, service):
     return np.array(lat)
 
 
-def serving_stream(rst, ctx, n_req, seed=4):
-    """Bounded mixed stream: receptors log-uniform 1k-20k atoms, ligands
-    20-80 atoms, 1-200 frames per request, Poisson arrivals at 70 % of the
-    one-at-a-time capacity; beside it the same requests one at a time (fused
-    engine, and plain FP64 form from its per-frame time on each system) on the
-    same arrival times."""
+def serving_stream(rst, ctx, n_req, n_systems=32, seed=4, load=0.7):
+    """Mixed MM-GBSA request stream: a pool of n_systems systems with
+    receptors log-uniform over 1k-20k atoms and ligands of 20-80 atoms; each
+    request takes a system of the pool and 1-200 frames (uniform); Poisson
+    arrivals at `load` of the one-at-a-time capacity.  Beside the continuous
+    batching loop: the same requests served one at a time in arrival order
+    through the fused engine (each request's service time measured alone)
+    and through the plain FP64 form (per-frame time of each system measured
+    on 2 frames), FIFO queues on the same arrival times."""
     S = _synthetic()
 
     rng = np.random.default_rng(seed)
     d = tempfile.mkdtemp()
     systems = []
-    for k in range(6):
+    for k in range(n_systems):
         nr = int(round(np.exp(rng.uniform(np.log(1000), np.log(20000)))))
         nl = int(rng.integers(20, 81))
         s = S.make_system(nr, nl, seed=3000 + k)
@@ -338,70 +349,74 @@ def serving_stream(rst, ctx, n_req, seed=4):
         kw = dict(gb_params=rst.GbParams(**GB), sa_params=rst.SaParams(n_sphere_points=NPTS), ctx=ctx)
         bs = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, **kw)
         bp = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, mode="plain", **kw)
-        systems.append((s, bs, bp, nr))
+        pool = S.make_frames(s, 200, seed=5000 + k)  # requests take slices of this pool
+        systems.append((s, bs, bp, nr + nl, pool))
     reqs = []
     for _ in range(n_req):
-        k = int(rng.integers(0, len(systems)))
-        reqs.append((k, S.make_frames(systems[k][0], int(rng.integers(1, 201)), seed=int(rng.integers(1 << 30)))))
-    for s, bs, bp, _ in systems:  # first-use preparation outside the stream
-        bs.run(S.make_frames(s, 1, seed=1))
-    # one request at a time through the fused engine (measured service times)
+        k = int(rng.integers(0, n_systems))
+        nf = int(rng.integers(1, 201))
+        a = int(rng.integers(0, 201 - nf))
+        reqs.append((k, a, nf))
+    frames_of = lambda k, a, nf: systems[k][4][a:a + nf]
+    for s, bs, bp, _, pool in systems:  # first-use preparation (layout, tuning) outside the stream
+        bs.run(pool[:1])
     svc = []
-    for k, fr in reqs:
+    for k, a, nf in reqs:  # one request at a time through the fused engine
         t = time.perf_counter()
-        systems[k][1].run(fr)
+        systems[k][1].run(frames_of(k, a, nf))
         svc.append(time.perf_counter() - t)
-    # Poisson arrivals at 70 % of the one-at-a-time capacity, so the queue is
-    # stable and latency measures scheduling rather than an overload backlog
-    mean_gap = sum(svc) / n_req / 0.7
+    mean_gap = sum(svc) / n_req / load
     arrivals = np.cumsum(rng.exponential(mean_gap, size=n_req))
     srv = rst.Server(max_inflight=4, ctx=ctx)
     t0 = time.perf_counter()
     ids = []
-    for (k, fr), a in zip(reqs, arrivals):
-        dt = a - (time.perf_counter() - t0)
+    for (k, a, nf), at in zip(reqs, arrivals):
+        dt = at - (time.perf_counter() - t0)
         if dt > 0:
             time.sleep(dt)
-        ids.append(srv.submit(systems[k][1], fr))
+        ids.append(srv.submit(systems[k][1], frames_of(k, a, nf)))
     for i in ids:
-        srv.wait(i, 600000)
+        srv.wait(i, 1200000)
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
-    frames = sum(fr.shape[0] for _, fr in reqs)
+    frames = sum(nf for _, _, nf in reqs)
     lat = _fifo_latencies(arrivals, svc)
-    # plain FP64 form: per-frame time of each system on 2 frames
     per_frame = []
-    for s, bs, bp, _ in systems:
-        f2 = S.make_frames(s, 3, seed=2)
-        bp.run(f2[:1])
+    for s, bs, bp, _, pool in systems:
+        bp.run(pool[:1])
         t = time.perf_counter()
-        bp.run(f2[1:])
+        bp.run(pool[1:3])
         per_frame.append((time.perf_counter() - t) / 2)
-    psvc = [per_frame[k] * fr.shape[0] for k, fr in reqs]
+    psvc = [per_frame[k] * nf for k, _, nf in reqs]
     plat = _fifo_latencies(arrivals, psvc)
-    return {"requests": n_req, "frames": frames, "receptor_atoms": [int(x[3]) for x in systems],
-            "continuous_batching": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+    atoms = sorted(int(x[3]) for x in systems)
+    return {"requests": n_req, "frames": frames, "systems": n_systems,
+            "complex_atoms_min_median_max": [atoms[0], atoms[len(atoms) // 2], atoms[-1]],
+            "continuous_batching": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
                                     "delivered_frames_per_s": frames / wall,
-                                    "note": "delivered rate follows the offered load (70 % of one-at-a-time capacity)"},
+                                    "note": "delivered rate follows the offered load"},
             "one_at_a_time_fused": {"p50_ms": 1e3 * float(np.percentile(lat, 50)),
                                     "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                                    "mean_ms": 1e3 * float(lat.mean()),
                                     "capacity_frames_per_s": frames / sum(svc)},
             "one_at_a_time_plain_fp64": {"p50_ms": 1e3 * float(np.percentile(plat, 50)),
                                          "p99_ms": 1e3 * float(np.percentile(plat, 99)),
                                          "capacity_frames_per_s": frames / sum(psvc),
                                          "how": "per-frame time of each system measured on 2 frames; FIFO queue "
                                                 "on the same arrival times"},
-            "arrival_mean_ms": 1e3 * mean_gap, "load": 0.7}
+            "arrival_mean_ms": 1e3 * mean_gap, "load": load}
 
 
-def large_mixed(rst, ctx, gb_requests=6, gb_frames=24, pb_requests=2, pb_frames=2, seed=5):
-    """Bounded large mixed load: 25,000 + 80 atoms, MM-GBSA (SASA 960 points)
-    and MM-PBSA (0.5 A grids of ~193^3, DH boundary) requests interleaved in
-    one serving loop; errors against the plain FP64 form on one frame."""
+def large_mixed(rst, ctx, n_frames=500, per_request=50, pb_rel_tol=1e-7, seed=5):
+    """25,000 + 80 atoms: MM-GBSA (SASA 960 points) and MM-PBSA (0.5 A grids of
+    ~193^3, DH boundary, relative-residual stop) requests of per_request
+    frames each, n_frames of each kind, interleaved in one serving loop with
+    Poisson gaps; throughput, latency percentiles, and the errors of frame 0
+    against the oracle's golden rows (accurate GB rows, converged PB rows)."""
     S = _synthetic()
 
-    s, fr = S.workload(5, n_frames=max(gb_frames, pb_frames) + 1)
+    s, fr = S.workload(5, n_frames=n_frames)
     d = tempfile.mkdtemp()
     S.write_prmtop(s, os.path.join(d, "w5.prmtop"))
     top = rst.read_prmtop(os.path.join(d, "w5.prmtop"))
@@ -410,35 +425,37 @@ def large_mixed(rst, ctx, gb_requests=6, gb_frames=24, pb_requests=2, pb_frames=
     pbkw = dict(pb_params=pbp, sa_params=rst.SaParams(n_sphere_points=NPTS), ctx=ctx)
     gsys = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, **gbkw)
     psys = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, **pbkw)
+    psys.set_pb_convergence(pb_rel_tol)
     gsys.run(fr[:1])
     psys.run(fr[:1])
     rng = np.random.default_rng(seed)
-    kinds = ["gb"] * gb_requests + ["pb"] * pb_requests
-    rng.shuffle(kinds)
+    starts = list(range(0, n_frames, per_request))
+    jobs = [("gb", a) for a in starts] + [("pb", a) for a in starts]
+    rng.shuffle(jobs)
     srv = rst.Server(max_inflight=4, ctx=ctx)
     t0 = time.perf_counter()
     ids = []
-    for k in kinds:
-        time.sleep(float(rng.exponential(0.02)))
-        ids.append((k, srv.submit(gsys if k == "gb" else psys, fr[1:1 + (gb_frames if k == "gb" else pb_frames)])))
-    outs = [(k, srv.wait(i, 1200000)) for k, i in ids]
+    for kind, a in jobs:
+        time.sleep(float(rng.exponential(0.05)))
+        ids.append((kind, a, srv.submit(gsys if kind == "gb" else psys, fr[a:a + per_request])))
+    outs = {(kind, a): srv.wait(i, 1800000) for kind, a, i in ids}
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
-    frames = sum(o.shape[0] for _, o in outs)
+    gb0, pb0 = outs[("gb", 0)][:1], outs[("pb", 0)][:1]
+    gold = _golden(5)
     err = {}
-    for k, sysk in (("gb", rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, mode="plain", **gbkw)),
-                    ("pb", rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, mode="plain", **pbkw))):
-        ref = sysk.run(fr[1:2])
-        got = next(o for kk, o in outs if kk == k)[:1]
-        err[k] = {"delta_polar": float(abs(got[0, 10] - ref[0, 10])), "delta_sa": float(abs(got[0, 11] - ref[0, 11])),
-                  "complex_polar": float(abs(got[0, 1] - ref[0, 1]))}
-    return {"atoms": int(s.n_atoms if hasattr(s, "n_atoms") else 25080), "gb_requests": gb_requests,
-            "gb_frames_per_request": gb_frames, "pb_requests": pb_requests, "pb_frames_per_request": pb_frames,
-            "frames": frames, "frames_per_s": frames / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "pb_stats": psys.pb_stats(), "abs_diff_vs_plain_fp64_frame1_kcal": err,
-            "note": "delta_mm of the plain form carries the reference's FP64 cancellation error (it subtracts "
-                    "sums of ~1e5 kcal/mol); polar and SA terms compared"}
+    if gold is not None:
+        cols = (("complex_polar", 1), ("receptor_polar", 4), ("ligand_polar", 7), ("delta_mm", 9),
+                ("delta_polar", 10), ("delta_sa", 11), ("delta_total", 12))
+        err["gb_vs_oracle_accurate"] = {k: float(abs(gb0[0, c] - gold["gb_accurate"][0][c])) for k, c in cols}
+        err["pb_vs_oracle_converged"] = {k: float(abs(pb0[0, c] - gold["pb_converged"][0][c])) for k, c in cols}
+        err["pb_oracle_reference_iterate_vs_converged"] = {
+            k: float(abs(gold["pb_faithful"][0][c] - gold["pb_converged"][0][c])) for k, c in cols}
+    return {"atoms": int(s.n_atoms), "gb_frames": n_frames, "pb_frames": n_frames, "frames_per_request": per_request,
+            "requests": len(jobs), "frames_per_s": 2 * n_frames / wall, "wall_s": wall,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "pb_rule": f"relative residual {pb_rel_tol:g}",
+            "pb_stats": psys.pb_stats(), "errors_frame0_kcal": err}
 
 
 def main():
@@ -451,15 +468,28 @@ def main():
     ap.add_argument("--frames", type=int, default=1000)
     ap.add_argument("--ref-frames", type=int, default=8)
     ap.add_argument("--plain-frames", type=int, default=16)
-    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-systems", type=int, default=32)
     ap.add_argument("--pb-frames", type=int, default=100, help="MM-PBSA leg frames (0: skip)")
     ap.add_argument("--pb-plain-frames", type=int, default=24, help="frames of the plain FP64 PB form")
     ap.add_argument("--no-large", action="store_true", help="skip the 25,080-atom mixed GB/PB serving leg")
     ap.add_argument("--pb-only", action="store_true", help="run only the MM-PBSA leg (--pb-frames frames) and print it")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the serving leg (--serve-requests over --serve-systems) and print it")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e/plain/cpu/serving legs")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.serve_only:
+        import torch
+
+        import rust_simulation_tools as rst
+        from rust_simulation_tools import _native as N
+
+        torch.cuda.set_device(0)
+        ctx = N.make_ctx(0, torch.cuda.current_stream().cuda_stream)
+        print(json.dumps(serving_stream(rst, ctx, args.serve_requests, args.serve_systems)), flush=True)
         return
     if args.pb_only:
         import torch
@@ -603,7 +633,7 @@ def main():
         if rank == 0 and world == 1 and args.ref_frames > 0:
             extras["cpu_baseline"] = cpu_baseline(s, fr, args.ref_frames, out_np, d_dec.cpu().numpy())
         if rank == 0 and world == 1 and args.serve_requests > 0:
-            extras["serving"] = serving_stream(rst, ctx, args.serve_requests)
+            extras["serving"] = serving_stream(rst, ctx, args.serve_requests, args.serve_systems)
         if rank == 0 and world == 1 and args.pb_frames > 0:
             # plain on the same frames
             extras["pbsa"] = pbsa_leg(rst, ctx, args.pb_frames, args.pb_plain_frames, hbm_peak())

@@ -396,8 +396,13 @@ typedef struct rstg_server_opts {
   int64_t memory_budget_bytes; /* limit on the batch buffers systems keep resident
                                   between requests; idle systems are evicted,
                                   least recently used first, to admit a request */
-  int32_t max_inflight;        /* requests running concurrently (device streams) */
-  int64_t chunk_frames;        /* frames per scheduling quantum                 */
+  int32_t max_inflight;        /* worker threads: requests with a chunk in flight */
+  int64_t chunk_frames;        /* frames per chunk (0: about 2.5e9 complex pair
+                                  evaluations for GB systems, 16 frames for PB,
+                                  8 in plain mode); chunks are dispatched oldest
+                                  request first, each on a stream whose priority
+                                  is its request's age rank among those in
+                                  flight                                        */
 } rstg_server_opts;
 void rstg_server_opts_default(rstg_server_opts* o);
 

@@ -81,7 +81,7 @@ rstg_frame_energy PlainFrameEval::run(const double* xc) {
       e[k].polar = v[7];
     } else {
       const Topology& t = sub[k].top;
-      e[k].polar = t.n_atoms ? pb_energy_run(ctx, hx[k], t.charges, t.radii, solv.pb, nullptr) : 0.0;
+      e[k].polar = t.n_atoms ? pb_energy_run(ctx, hx[k], t.charges, t.radii, solv.pb, nullptr, pb_rel_tol) : 0.0;
     }
     e[k].sa = sa.surface_tension * v[8] + sa.offset;
   }

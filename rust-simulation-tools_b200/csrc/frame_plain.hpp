@@ -10,7 +10,8 @@ namespace rstg {
 // PB polar energy of one (sub)system (pb_energy.rs:332-438), pb.cu.  xyz_host
 // is Angstrom [n][3]; charges in e.
 double pb_energy_run(Ctx* c, const std::vector<double>& xyz_host, const std::vector<double>& q_e,
-                     const std::vector<double>& radii, const rstg_pb_params& p, rstg_pb_diag* diag);
+                     const std::vector<double>& radii, const rstg_pb_params& p, rstg_pb_diag* diag,
+                     double rtol);
 
 struct PlainSub {
   Topology top;
@@ -26,6 +27,7 @@ struct PlainFrameEval {
   DevBuf sphere, xyz[3], born, per_atom, out, overflow, rec_idx, lig_idx;
   int64_t n_sphere = 0;
   Ctx* ctx = nullptr;
+  double pb_rel_tol = 0.0;  // > 0: PB grids solved to this relative residual (not the reference's rule)
 
   PlainFrameEval(Ctx* c, const Topology& t, const std::vector<int64_t>& rres, const std::vector<int64_t>& lres,
                  const rstg_solvation& solv, const rstg_sa_params& sa);

@@ -624,11 +624,14 @@ __global__ void k_restrict(const double* __restrict__ f, int fnx, int fny, int f
   c[i] = scale * sum / ws;
 }
 
+// skipb (relative-residual mode): corrections vanish on the boundary, so
+// boundary points are left alone
 __global__ void k_prolong(const double* __restrict__ c, int cnx, int cny, int cnz, double* __restrict__ f, int fnx,
-                          int fny, int fnz) {
+                          int fny, int fnz, int skipb) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)fnx * fny * fnz) return;
   int fz = (int)(i / ((long long)fnx * fny)), fy = (int)((i / fnx) % fny), fx = (int)(i % fnx);
+  if (skipb && (fx == 0 || fy == 0 || fz == 0 || fx == fnx - 1 || fy == fny - 1 || fz == fnz - 1)) return;
   double cxf = (double)fx / 2.0, cyf = (double)fy / 2.0, czf = (double)fz / 2.0;
   int mx = cnx >= 2 ? cnx - 2 : 0, my = cny >= 2 ? cny - 2 : 0, mz = cnz >= 2 ? cnz - 2 : 0;
   int x0 = min((int)floor(cxf), mx), y0 = min((int)floor(cyf), my), z0 = min((int)floor(czf), mz);
@@ -649,6 +652,40 @@ __global__ void k_coarsen(const double* __restrict__ f, int fnx, int fny, int fn
   int cz = (int)(i / ((long long)cnx * cny)), cy = (int)((i / cnx) % cny), cx = (int)(i % cnx);
   int fx = min(2 * cx, fnx - 1), fy = min(2 * cy, fny - 1), fz = min(2 * cz, fnz - 1);
   c[i] = f[fx + (long long)fnx * (fy + (long long)fny * fz)];
+}
+
+// Coarse face dielectric of the relative-residual mode: two fine faces in
+// series along the face's axis (harmonic mean; equal values copied), the
+// 3 x 3 neighbouring lines across it in parallel (weights 1-2-1 per
+// transverse direction, renormalised at the grid edge).
+__global__ void k_coarsen_face(const double* __restrict__ f, int fnx, int fny, int fnz, double* __restrict__ c,
+                               int cnx, int cny, int cnz, int axis) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)cnx * cny * cnz) return;
+  int cz = (int)(i / ((long long)cnx * cny)), cy = (int)((i / cnx) % cny), cx = (int)(i % cnx);
+  const int n[3] = {fnx, fny, fnz};
+  const int b[3] = {min(2 * cx, fnx - 1), min(2 * cy, fny - 1), min(2 * cz, fnz - 1)};
+  const int t1 = axis == 0 ? 1 : 0, t2 = axis == 2 ? 1 : 2;
+  double sum = 0.0, ws = 0.0, first = 0.0;
+  bool same = true, any = false;
+  for (int u = -1; u <= 1; u++)
+    for (int v = -1; v <= 1; v++) {
+      int p[3] = {b[0], b[1], b[2]};
+      p[t1] += u;
+      p[t2] += v;
+      if (p[t1] < 0 || p[t1] >= n[t1] || p[t2] < 0 || p[t2] >= n[t2]) continue;
+      int q[3] = {p[0], p[1], p[2]};
+      q[axis] = min(p[axis] + 1, n[axis] - 1);
+      const double e0 = f[p[0] + (long long)fnx * (p[1] + (long long)fny * p[2])];
+      const double e1 = f[q[0] + (long long)fnx * (q[1] + (long long)fny * q[2])];
+      if (!any) first = e0;
+      any = true;
+      same = same && e0 == first && e1 == first;
+      const double w = (u == 0 ? 2.0 : 1.0) * (v == 0 ? 2.0 : 1.0);
+      sum += w * (e0 == e1 ? e0 : 2.0 / (1.0 / e0 + 1.0 / e1));
+      ws += w;
+    }
+  c[i] = same ? first : sum / ws;
 }
 
 // coarsest level: 50 red-black sweeps in one block (same arithmetic as k_rb)
@@ -909,13 +946,17 @@ static LevelDev ldev(const PbGeom& g, const double* ex, const double* ey, const 
   return LevelDev{g.nx, g.ny, g.nz, ih, ih, ih, ex, ey, ez, k2};
 }
 
+// rel: the relative-residual mode's consistent multigrid (Gauss-Seidel
+// smoothing, restriction without the 0.25 factor, series/parallel coarse
+// dielectrics, corrections zero on the boundary) instead of the reference's.
 struct Solver {
   Ctx* c;
   cudaStream_t st;
   MapsView M;
   std::vector<MgLevel> L;
   DevBuf part, scal;
-  Solver(Ctx* cc, const MapsView& m) : c(cc), st(pb_stream(cc)), M(m) {
+  bool rel = false;
+  Solver(Ctx* cc, const MapsView& m, bool relative = false) : c(cc), st(pb_stream(cc)), M(m), rel(relative) {
     size_t parts = (size_t)nblk(m.g.nx, 128) * std::max(m.g.ny - 2, 1) * std::max(m.g.nz - 2, 1);
     part = DevBuf(std::max<size_t>(parts, 1) * 8, st);
     scal = DevBuf(64, st);
@@ -937,10 +978,14 @@ struct Solver {
       const double* src[4] = {ex, ey, ez, k2};
       DevBuf* dst[4] = {&lv.ex, &lv.ey, &lv.ez, &lv.k2};
       for (int k = 0; k < 4; k++)
-        k_coarsen<<<nblk(cn, 256), 256, 0, st>>>(src[k], g.nx, g.ny, g.nz, dst[k]->as<double>(), lv.g.nx, lv.g.ny,
-                                                 lv.g.nz);
+        if (rel && k < 3)
+          k_coarsen_face<<<nblk(cn, 256), 256, 0, st>>>(src[k], g.nx, g.ny, g.nz, dst[k]->as<double>(), lv.g.nx,
+                                                        lv.g.ny, lv.g.nz, k);
+        else
+          k_coarsen<<<nblk(cn, 256), 256, 0, st>>>(src[k], g.nx, g.ny, g.nz, dst[k]->as<double>(), lv.g.nx, lv.g.ny,
+                                                   lv.g.nz);
       launched(c, 4);
-      lv.omega = pb_omega(lv.g.nx, lv.g.ny, lv.g.nz);
+      lv.omega = rel ? 1.0 : pb_omega(lv.g.nx, lv.g.ny, lv.g.nz);
       L.push_back(std::move(lv));
       MgLevel& b = L.back();
       ex = b.ex.as<double>();
@@ -1000,12 +1045,13 @@ struct Solver {
     }
     long long cn = (long long)lv.g.n();
     k_restrict<<<nblk(cn, 256), 256, 0, st>>>(lv.res.as<double>(), g.nx, g.ny, g.nz, lv.rhs.as<double>(), lv.g.nx,
-                                              lv.g.ny, lv.g.nz, 0.25);
+                                              lv.g.ny, lv.g.nz, rel ? 1.0 : 0.25);
     RSTG_CUDA(cudaMemsetAsync(lv.corr.p, 0, cn * 8, st));
     launched(c);
     LevelDev cl = ldev(lv.g, lv.ex.as<double>(), lv.ey.as<double>(), lv.ez.as<double>(), lv.k2.as<double>());
     v_cycle(lvl + 1, lv.g, cl, lv.corr.as<double>(), lv.rhs.as<double>(), lv.omega, 1.0);
-    k_prolong<<<nblk(fn, 256), 256, 0, st>>>(lv.corr.as<double>(), lv.g.nx, lv.g.ny, lv.g.nz, phi, g.nx, g.ny, g.nz);
+    k_prolong<<<nblk(fn, 256), 256, 0, st>>>(lv.corr.as<double>(), lv.g.nx, lv.g.ny, lv.g.nz, phi, g.nx, g.ny, g.nz,
+                                             rel ? 1 : 0);
     launched(c);
     smooth(ld, phi, rho, omega, 3, rs, nullptr);
   }
@@ -1040,8 +1086,12 @@ static void apply_bc(Ctx* c, const PbGeom& g, double* phi, const AtomsDev& A, co
 }
 
 // solve_lpbe_multigrid (pb_solver.rs:1015-1167) with the plain SOR fallback
-// (pb_solver.rs:373-447)
-static SolveOut solve_mg(Ctx* c, const MapsView& M, const AtomsDev& A, const BcSpec& bc, double tol, int64_t maxit) {
+// (pb_solver.rs:373-447).  rtol > 0: the relative-residual mode -- the
+// consistent multigrid, stopping when the RMS residual falls below rtol times
+// its initial value (SOR grids: the residual after each sweep); the
+// reference's cycle cap and divergence rule stay.
+static SolveOut solve_mg(Ctx* c, const MapsView& M, const AtomsDev& A, const BcSpec& bc, double tol, int64_t maxit,
+                         double rtol = 0.0) {
   cudaStream_t st = pb_stream(c);
   const PbGeom& g = M.g;
   long long n = (long long)g.n();
@@ -1049,8 +1099,10 @@ static SolveOut solve_mg(Ctx* c, const MapsView& M, const AtomsDev& A, const BcS
   R.phi = DevBuf(n * 8, st);
   RSTG_CUDA(cudaMemsetAsync(R.phi.p, 0, n * 8, st));
   apply_bc(c, g, R.phi.as<double>(), A, bc);
-  Solver S(c, M);
+  const bool rel = rtol > 0.0;
+  Solver S(c, M, rel);
   LevelDev top = ldev(g, M.ex, M.ey, M.ez, M.k2);
+  const double r0 = rel ? S.rms_residual(top, R.phi.as<double>(), M.rho, kFourPiEc) : 0.0;
   auto sor = [&](bool restart) {
     if (restart) RSTG_CUDA(cudaMemsetAsync(R.phi.p, 0, n * 8, st));
     apply_bc(c, g, R.phi.as<double>(), A, bc);
@@ -1060,10 +1112,11 @@ static SolveOut solve_mg(Ctx* c, const MapsView& M, const AtomsDev& A, const BcS
     for (int64_t it = 0; it < maxit; it++) {
       double rms = 0.0;
       S.smooth(top, R.phi.as<double>(), M.rho, om, 1, kFourPiEc, &rms);
+      if (rel) rms = S.rms_residual(top, R.phi.as<double>(), M.rho, kFourPiEc) / std::max(r0, 1e-300);
       R.residual = rms;
       R.iterations = it + 1;
       om = it == 0 ? 1.0 / (1.0 - rs2 / 2.0) : 1.0 / (1.0 - rs2 * om / 4.0);
-      if (rms < tol) {
+      if (rms < (rel ? rtol : tol)) {
         R.converged = true;
         return;
       }
@@ -1076,7 +1129,7 @@ static SolveOut solve_mg(Ctx* c, const MapsView& M, const AtomsDev& A, const BcS
   }
   int64_t maxv = std::min<int64_t>(std::max<int64_t>(maxit / 6, 1), 200);
   S.build_levels();
-  double omega = pb_omega(g.nx, g.ny, g.nz);
+  double omega = rel ? 1.0 : pb_omega(g.nx, g.ny, g.nz);
   double best = std::numeric_limits<double>::max(), prev = std::numeric_limits<double>::max();
   int growing = 0;
   for (int64_t cyc = 0; cyc < maxv; cyc++) {
@@ -1094,14 +1147,14 @@ static SolveOut solve_mg(Ctx* c, const MapsView& M, const AtomsDev& A, const BcS
       return R;
     }
     prev = r;
-    if (r < tol) {
+    if (rel ? r < rtol * r0 : r < tol) {
       R.iterations = cyc + 1;
-      R.residual = r;
+      R.residual = rel ? r / std::max(r0, 1e-300) : r;
       R.converged = true;
       return R;
     }
   }
-  R.residual = S.rms_residual(top, R.phi.as<double>(), M.rho, kFourPiEc);
+  R.residual = S.rms_residual(top, R.phi.as<double>(), M.rho, kFourPiEc) / (rel ? std::max(r0, 1e-300) : 1.0);
   R.iterations = maxv;
   R.converged = false;
   return R;
@@ -1132,7 +1185,7 @@ static double maxabs(Ctx* c, const DevBuf& phi, long long n) {
 
 // pb_solve_with_focusing, pb_energy.rs:134-322
 static double solve_focus(Ctx* c, const Maps& fine_rho, const PbGeom* cg, const AtomsDev& A, const rstg_pb_params& p,
-                          double ein, double eout, double kap, bool ionic, SolveOut* out) {
+                          double ein, double eout, double kap, bool ionic, SolveOut* out, double rtol) {
   double bck = ionic ? kap : 0.0;
   BcSpec dh;
   dh.kind = 1;
@@ -1151,20 +1204,20 @@ static double solve_focus(Ctx* c, const Maps& fine_rho, const PbGeom* cg, const 
     charge_map(c, *cg, A, C.rho);
     dielectric_maps(c, C, A, p.probe_radius, ein, eout);
     kappa_map(c, C, A, p.ion_radius, kap, p.solvent_dielectric, ionic);
-    SolveOut cr = solve_mg(c, C.view(), A, dh, p.tolerance * 10.0, p.max_iterations);
+    SolveOut cr = solve_mg(c, C.view(), A, dh, p.tolerance * 10.0, p.max_iterations, rtol);
     double mp = maxabs(c, cr.phi, (long long)cg->n());
     bool ok = cr.converged && std::isfinite(mp) && mp < 1e10;
     fine_maps(F);
     F.rho = DevBuf(fine_rho.g.n() * 8, pb_stream(c));
     RSTG_CUDA(cudaMemcpyAsync(F.rho.p, fine_rho.rho.p, fine_rho.g.n() * 8, cudaMemcpyDeviceToDevice, pb_stream(c)));
     if (!ok) {
-      *out = solve_mg(c, F.view(), A, dh, p.tolerance, p.max_iterations);
+      *out = solve_mg(c, F.view(), A, dh, p.tolerance, p.max_iterations, rtol);
     } else {
       BcSpec ib;
       ib.kind = 2;
       ib.cg = cg;
       ib.cphi = cr.phi.as<double>();
-      *out = solve_mg(c, F.view(), A, ib, p.tolerance, p.max_iterations);
+      *out = solve_mg(c, F.view(), A, ib, p.tolerance, p.max_iterations, rtol);
       RSTG_CUDA(cudaStreamSynchronize(pb_stream(c)));
     }
     return elec_energy(c, F.g, out->phi.as<double>(), A);
@@ -1172,7 +1225,7 @@ static double solve_focus(Ctx* c, const Maps& fine_rho, const PbGeom* cg, const 
   fine_maps(F);
   F.rho = DevBuf(fine_rho.g.n() * 8, pb_stream(c));
   RSTG_CUDA(cudaMemcpyAsync(F.rho.p, fine_rho.rho.p, fine_rho.g.n() * 8, cudaMemcpyDeviceToDevice, pb_stream(c)));
-  *out = solve_mg(c, F.view(), A, dh, p.tolerance, p.max_iterations);
+  *out = solve_mg(c, F.view(), A, dh, p.tolerance, p.max_iterations, rtol);
   return elec_energy(c, F.g, out->phi.as<double>(), A);
 }
 
@@ -1254,7 +1307,7 @@ void pb_grid_maps(Ctx* c, const std::vector<double>& x, const std::vector<double
 }
 
 double pb_energy_run(Ctx* c, const std::vector<double>& x, const std::vector<double>& q,
-                     const std::vector<double>& radii, const rstg_pb_params& p, rstg_pb_diag* diag) {
+                     const std::vector<double>& radii, const rstg_pb_params& p, rstg_pb_diag* diag, double rtol) {
   if (!(p.grid_spacing > 0.0)) throw Error(RSTG_ERR_INVALID, "grid_spacing must be positive");
   if (q.empty()) return 0.0;
   double s = p.salt_concentration;
@@ -1269,8 +1322,10 @@ double pb_energy_run(Ctx* c, const std::vector<double>& x, const std::vector<dou
   if (focus) cg = pb_coarse_grid(x, p.grid_spacing, p.fillratio, p.fscale);
   charge_map(c, fine.g, A, fine.rho);
   SolveOut rs, rr;
-  double es = solve_focus(c, fine, focus ? &cg : nullptr, A, p, p.solute_dielectric, p.solvent_dielectric, kap, true, &rs);
-  double er = solve_focus(c, fine, focus ? &cg : nullptr, A, p, p.solute_dielectric, p.solute_dielectric, kap, false, &rr);
+  double es = solve_focus(c, fine, focus ? &cg : nullptr, A, p, p.solute_dielectric, p.solvent_dielectric, kap, true,
+                          &rs, rtol);
+  double er = solve_focus(c, fine, focus ? &cg : nullptr, A, p, p.solute_dielectric, p.solute_dielectric, kap, false,
+                          &rr, rtol);
   if (diag) {
     diag->iterations[0] = rs.iterations;
     diag->iterations[1] = rr.iterations;

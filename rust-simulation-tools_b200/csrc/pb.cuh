@@ -89,7 +89,8 @@ PbSolveStats pb_solve_fp64(Ctx* c, const PbGeom& g, const double* rho, const dou
 
 // One paired PB energy (solvated - reference) of one (sub)system.
 double pb_energy_run(Ctx* c, const std::vector<double>& xyz_host, const std::vector<double>& q_e,
-                     const std::vector<double>& radii, const rstg_pb_params& p, rstg_pb_diag* diag);
+                     const std::vector<double>& radii, const rstg_pb_params& p, rstg_pb_diag* diag,
+                     double rtol = 0.0);
 
 // Grid set-up of one solve (for inspection and tests): dims/origin always;
 // with charge != NULL every map of that solve and the boundary potential.

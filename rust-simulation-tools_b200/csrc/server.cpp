@@ -1,8 +1,14 @@
 // Serving loop: requests of different systems and frame counts arrive while
-// others run; a dispatcher admits them into free slots when the device-memory
-// budget allows (footprint of the request's batch buffers), each slot runs its
-// request on its own CUDA stream so work of several requests overlaps on the
-// device, and per-request latency (submit -> results ready) is recorded.
+// others run.  Each request is cut into chunks of frames; worker threads
+// (max_inflight of them) take chunks oldest request first, so at most one
+// chunk of a request -- and of a system -- runs at a time, the device-memory
+// budget admits a request's first chunk (footprint of its batch buffers), and
+// work of several requests overlaps on the device.  A chunk runs on a stream
+// whose priority is its request's age rank among the requests in flight (the
+// oldest on the highest priority): the device hands freed SMs to the oldest
+// request's blocks first, so a large request is not stretched by the small
+// ones that fill the gaps, and at every chunk boundary the ranks are taken
+// again.  Per-request latency (submit -> results ready) is recorded.
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -28,6 +34,11 @@ struct Request {
   int64_t n_frames = 0;
   std::vector<rstg_frame_energy> out;
   int64_t bytes = 0;
+  int64_t chunk = 1;     // frames per chunk
+  int64_t next = 0;      // first frame not yet dispatched
+  int64_t done = 0;      // frames finished
+  bool in_flight = false;
+  bool admitted = false;  // its buffers are counted in the resident bytes
   Clock::time_point submitted, finished;
   enum State { QUEUED, RUNNING, DONE, FAILED, CANCELLED } state = QUEUED;
   rstg_status err = RSTG_OK;
@@ -39,11 +50,12 @@ struct Server {
   rstg_server_opts opts;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<std::shared_ptr<Request>> queue;
+  std::deque<std::shared_ptr<Request>> queue;  // unfinished requests in submission order
   std::map<int64_t, std::shared_ptr<Request>> all;
   std::vector<std::thread> slots;
-  std::vector<cudaStream_t> streams;
-  std::map<System*, int> busy;  // systems with a running request
+  std::vector<std::vector<cudaStream_t>> streams;  // [worker][priority level], level 0 the highest
+  int prio_hi = 0, prio_lo = 0;
+  std::map<System*, int> busy;  // systems with a chunk in flight
   // Device bytes each system holds between requests (its batch buffers stay
   // resident so that its next request reuses them and its captured graph);
   // idle systems are evicted, least recently used first, when an admission
@@ -65,41 +77,44 @@ struct Server {
     size_t fr = 0, tot = 0;
     RSTG_CUDA(cudaMemGetInfo(&fr, &tot));
     device_bytes = (int64_t)tot;
-    streams = take_streams(c->device, n);
+    RSTG_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));  // (least, greatest)
+    int levels = std::min(n, prio_lo - prio_hi + 1);
+    for (int k = 0; k < n; k++) {
+      std::vector<cudaStream_t> per;
+      for (int l = 0; l < levels; l++) per.push_back(take_stream(c->device, prio_hi + l));
+      streams.push_back(per);
+    }
     for (int k = 0; k < n; k++) slots.emplace_back([this, k] { slot_loop(k); });
   }
 
-  // Slot streams come from a per-device pool and are never destroyed: a
-  // system that grew device buffers during a request frees them later with
-  // cudaFreeAsync on the stream they were allocated on, which must still
-  // exist then, whenever the system is destroyed.
+  // Streams come from a per-device, per-priority pool and are never
+  // destroyed: a system that grew device buffers during a request frees them
+  // later with cudaFreeAsync on the stream they were allocated on, which must
+  // still exist then, whenever the system is destroyed.
   static std::mutex& pool_mu() {
     static std::mutex m;
     return m;
   }
-  static std::map<int, std::vector<cudaStream_t>>& pool() {
-    static auto* p = new std::map<int, std::vector<cudaStream_t>>();
+  static std::map<std::pair<int, int>, std::vector<cudaStream_t>>& pool() {
+    static auto* p = new std::map<std::pair<int, int>, std::vector<cudaStream_t>>();
     return *p;
   }
-  static std::vector<cudaStream_t> take_streams(int device, int n) {
+  static cudaStream_t take_stream(int device, int prio) {
     std::lock_guard<std::mutex> lk(pool_mu());
-    std::vector<cudaStream_t>& free = pool()[device];
-    std::vector<cudaStream_t> out;
-    while ((int)out.size() < n && !free.empty()) {
-      out.push_back(free.back());
+    std::vector<cudaStream_t>& free = pool()[{device, prio}];
+    if (!free.empty()) {
+      cudaStream_t s = free.back();
       free.pop_back();
+      return s;
     }
-    while ((int)out.size() < n) {
-      cudaStream_t s;
-      RSTG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-      out.push_back(s);
-    }
-    return out;
+    cudaStream_t s;
+    RSTG_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio));
+    return s;
   }
-  static void give_streams(int device, const std::vector<cudaStream_t>& s) {
+  void give_streams() {
     std::lock_guard<std::mutex> lk(pool_mu());
-    auto& free = pool()[device];
-    free.insert(free.end(), s.begin(), s.end());
+    for (auto& per : streams)
+      for (size_t l = 0; l < per.size(); l++) pool()[{ctx->device, prio_hi + (int)l}].push_back(per[l]);
   }
 
   ~Server() {
@@ -110,8 +125,26 @@ struct Server {
     cv_work.notify_all();
     for (auto& t : slots) t.join();
     ctx->bind();
-    for (auto s : streams) cudaStreamSynchronize(s);
-    give_streams(ctx->device, streams);
+    for (auto& per : streams)
+      for (auto st : per) cudaStreamSynchronize(st);
+    give_streams();
+  }
+
+  // Frames per chunk: about 2.5e9 complex pair evaluations (some 20 ms of
+  // device time whatever the system size) for the GB engine, 16 frames for
+  // the batched PB engine (its lock-step cycles have a fixed cost per batch),
+  // 8 frames in plain mode; opts.chunk_frames > 0 overrides.
+  int64_t chunk_for(const System* sys, int64_t F) const {
+    int64_t c;
+    if (opts.chunk_frames > 0)
+      c = opts.chunk_frames;
+    else if (sys->opts.mode != RSTG_MODE_FUSED)
+      c = 8;
+    else if (sys->solv.method == 1)
+      c = 16;
+    else
+      c = (int64_t)(2.5e9 / std::max(1.0, (double)sys->nC * (double)sys->nC));
+    return std::max<int64_t>(1, std::min(c, std::max<int64_t>(F, 1)));
   }
 
   int64_t growth(const Request& r) {
@@ -126,7 +159,12 @@ struct Server {
   void evict_for(int64_t need, System* keep) {
     std::vector<std::pair<int64_t, System*>> order;
     for (auto& kv : resident)
-      if (kv.first != keep && !busy.count(kv.first)) order.push_back({last_use[kv.first], kv.first});
+      if (kv.first != keep && !busy.count(kv.first)) {
+        bool pending = false;  // a system with an admitted, unfinished request keeps its buffers
+        for (auto& q : queue)
+          if (q->sys == kv.first && q->admitted) pending = true;
+        if (!pending) order.push_back({last_use[kv.first], kv.first});
+      }
     std::sort(order.begin(), order.end());
     for (auto& o : order) {
       if (resident_total + need <= opts.memory_budget_bytes) return;
@@ -140,81 +178,103 @@ struct Server {
     }
   }
 
-  // Next admissible request: first in arrival order whose system is idle and
-  // whose buffers fit the budget after evicting idle systems (a request
-  // larger than the whole budget is admitted alone when nothing else runs,
-  // so it cannot starve).
+  // Next chunk to run: of the oldest request that has frames left, no chunk
+  // in flight and an idle system; a request's first chunk also needs its
+  // buffers to fit the budget after evicting idle systems (a request larger
+  // than the whole budget is admitted alone when nothing else runs, so it
+  // cannot starve).
   std::shared_ptr<Request> pick() {
-    for (auto it = queue.begin(); it != queue.end(); ++it) {
-      auto& r = *it;
+    for (auto& r : queue) {
+      if (r->in_flight || r->next >= r->n_frames || r->state == Request::CANCELLED) continue;
       if (busy.count(r->sys)) continue;
-      int64_t need = growth(*r);
-      evict_for(need, r->sys);
-      bool fits = resident_total + need <= opts.memory_budget_bytes || running == 0;
-      if (!fits) continue;
-      auto q = r;
-      queue.erase(it);
-      return q;
+      if (!r->admitted) {
+        int64_t need = growth(*r);
+        evict_for(need, r->sys);
+        if (!(resident_total + need <= opts.memory_budget_bytes || running == 0)) continue;
+        resident[r->sys] += need;
+        resident_total += need;
+        peak_bytes = std::max(peak_bytes, resident_total);
+        r->admitted = true;
+      }
+      return r;
     }
     return nullptr;
+  }
+
+  void finish(const std::shared_ptr<Request>& r) {  // with mu held
+    r->finished = Clock::now();
+    queue.erase(std::remove(queue.begin(), queue.end(), r), queue.end());
+    r->frames.clear();
+    r->frames.shrink_to_fit();
   }
 
   void slot_loop(int k) {
     cudaSetDevice(ctx->device);
     for (;;) {
       std::shared_ptr<Request> r;
+      int64_t f0 = 0, B = 0;
+      cudaStream_t st = nullptr;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv_work.wait(lk, [&] { return stop || (r = pick()) != nullptr; });
         if (!r) return;
-        r->state = Request::RUNNING;
+        if (r->state == Request::QUEUED) r->state = Request::RUNNING;
+        r->in_flight = true;
         busy[r->sys] = 1;
-        int64_t g = growth(*r);
-        resident[r->sys] += g;
-        resident_total += g;
         last_use[r->sys] = ++use_clock;
-        peak_bytes = std::max(peak_bytes, resident_total);
         running++;
+        f0 = r->next;
+        B = std::min(r->chunk, r->n_frames - f0);
+        r->next += B;
+        int rank = 0;  // requests older than r with a chunk in flight
+        for (auto& q : queue) {
+          if (q == r) break;
+          if (q->in_flight) rank++;
+        }
+        st = streams[k][std::min<int>(rank, (int)streams[k].size() - 1)];
       }
-      rstg_status st = RSTG_OK;
+      rstg_status code = RSTG_OK;
       std::string msg;
       try {
         std::lock_guard<std::recursive_mutex> sl(r->sys->mu);
         cudaStream_t prev = r->sys->stream_;
-        if (r->sys->opts.mode == RSTG_MODE_FUSED) r->sys->stream_ = streams[k];
+        if (r->sys->opts.mode == RSTG_MODE_FUSED) r->sys->stream_ = st;
         try {
-          r->sys->run(r->frames.data(), false, true, r->n_frames, r->out.data(), true, nullptr);
+          r->sys->run(r->frames.data() + (size_t)f0 * r->sys->n_top * 3, false, true, B, r->out.data() + f0, true,
+                      nullptr);
         } catch (...) {
           r->sys->stream_ = prev;
           throw;
         }
         r->sys->stream_ = prev;
       } catch (const Error& e) {
-        st = e.code;
+        code = e.code;
         msg = e.what();
       } catch (const std::exception& e) {
-        st = RSTG_ERR_INVALID;
+        code = RSTG_ERR_INVALID;
         msg = e.what();
       }
       {
         std::lock_guard<std::mutex> lk(mu);
-        r->finished = Clock::now();
         busy.erase(r->sys);
         running--;
+        r->in_flight = false;
+        r->done += B;
         if (r->state == Request::CANCELLED) {
           r->out.clear();
-        } else if (st != RSTG_OK) {
+          finish(r);
+        } else if (code != RSTG_OK) {
           r->state = Request::FAILED;
-          r->err = st;
+          r->err = code;
           r->msg = msg;
-        } else {
+          finish(r);
+        } else if (r->done == r->n_frames) {
           r->state = Request::DONE;
+          finish(r);
           latencies_ms.push_back(std::chrono::duration<double, std::milli>(r->finished - r->submitted).count());
           frames_done += r->n_frames;
           last_done = r->finished;
         }
-        r->frames.clear();
-        r->frames.shrink_to_fit();
       }
       cv_done.notify_all();
       cv_work.notify_all();
@@ -227,7 +287,8 @@ struct Server {
     r->n_frames = F;
     r->frames.assign(frames, frames + (size_t)F * sys->n_top * 3);
     r->out.resize(F);
-    r->bytes = sys->footprint(std::min<int64_t>(F, sys->batch > 0 ? sys->batch : F));
+    r->chunk = chunk_for(sys, F);
+    r->bytes = sys->footprint(std::min<int64_t>(r->chunk, sys->batch > 0 ? sys->batch : r->chunk));
     if (r->bytes > device_bytes)
       throw Error(RSTG_ERR_NOMEM, "request needs " + std::to_string(r->bytes) + " bytes of device memory; the device has " +
                                       std::to_string(device_bytes));
@@ -238,8 +299,15 @@ struct Server {
       first_submit = r->submitted;
       any = true;
     }
-    queue.push_back(r);
     all[r->id] = r;
+    if (F == 0) {  // nothing to evaluate
+      r->state = Request::DONE;
+      r->finished = r->submitted;
+      latencies_ms.push_back(0.0);
+      cv_done.notify_all();
+      return r->id;
+    }
+    queue.push_back(r);
     cv_work.notify_all();
     return r->id;
   }
@@ -348,14 +416,13 @@ rstg_status rstg_server_cancel(rstg_server* s, int64_t id) {
   try {
     std::lock_guard<std::mutex> lk(s->mu);
     auto r = s->find(id);
-    if (r->state == Request::QUEUED) {
-      s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), r), s->queue.end());
-      r->frames.clear();
-      r->state = Request::CANCELLED;
-      r->finished = Clock::now();
-      s->cv_done.notify_all();
-    } else if (r->state == Request::RUNNING) {
-      r->state = Request::CANCELLED;  // results are discarded when the run ends
+    if (r->state == Request::QUEUED || r->state == Request::RUNNING) {
+      r->state = Request::CANCELLED;  // no further chunk is dispatched
+      if (!r->in_flight) {            // else the chunk's worker finishes it when the chunk ends
+        r->out.clear();
+        s->finish(r);
+        s->cv_done.notify_all();
+      }
     }
     return RSTG_OK;
   } catch (const Error& e) {

@@ -1293,10 +1293,12 @@ static std::mutex g_tune_mu;
 static std::map<TuneKey, std::pair<int, int>> g_tuned;
 
 // Times every launch shape of k_pairs and k_sasa on the first frames of the
-// first run (inputs already in in_frames; one warm pass fills the buffers
-// they read) and keeps the fastest of each: best of two CUDA-event timed
-// launches on the system stream.
-void System::tune(bool f64, int64_t B) {
+// first run and keeps the fastest of each: best of two CUDA-event timed
+// launches on the system stream.  The tuning batch holds enough frames for
+// at least 2,048 pair-kernel blocks (the first run's frames repeated when it
+// has fewer), at most 64 or the batch size; one warm pass fills the buffers
+// the timed kernels read.
+void System::tune(const void* frames, bool f64, bool host_in, int64_t F) {
   TuneKey key{ctx->device, nC, nR, fp->npts};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1309,7 +1311,16 @@ void System::tune(bool f64, int64_t B) {
     }
   }
   cudaStream_t st = stream();
-  int64_t TB = std::min<int64_t>(B, 64);
+  const int64_t B = std::min(F, batch);
+  int64_t TB = std::min<int64_t>(batch, std::max<int64_t>(std::min<int64_t>(B, 64), (2048 + fp->ntiles - 1) / fp->ntiles));
+  TB = std::max<int64_t>(TB, 1);
+  ensure_buffers(TB);
+  const size_t fb = (size_t)n_top * 3 * (f64 ? 8 : 4);
+  const int64_t nb = std::min(B, TB);
+  RSTG_CUDA(cudaMemcpyAsync(in_frames.p, frames, nb * fb, host_in ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+  for (int64_t f = nb; f < TB; f++)
+    RSTG_CUDA(cudaMemcpyAsync((char*)in_frames.p + f * fb, (const char*)in_frames.p + (f % nb) * fb, fb,
+                              cudaMemcpyDeviceToDevice, st));
   launch_batch(in_frames.p, f64, TB, res_buf.as<rstg_frame_energy>(), nullptr);
   cudaEvent_t a, b;
   RSTG_CUDA(cudaEventCreate(&a));
@@ -1525,6 +1536,7 @@ void System::run_plain(const void* frames, bool f64, bool host_in, int64_t F, rs
   int64_t nres = n_res_rec + n_res_lig;
   std::vector<rstg_residue_energy> dres(decomp ? F * nres : 0);
   int64_t before = ctx->launches.load();
+  plain->pb_rel_tol = pb_rel_tol;
   for (int64_t f = 0; f < F; f++) {
     std::vector<double> xc(nC * 3);
     for (int64_t a = 0; a < nC; a++) {
@@ -1652,12 +1664,7 @@ void System::run(const void* frames, bool f64, bool host_in, int64_t F, rstg_fra
   int64_t nres = fp->nres;
   for (int attempt = 0; attempt < 3; attempt++) {
     ensure_buffers(std::min(F, batch));
-    if (!tuned && opts.autotune) {
-      int64_t B = std::min(batch, F);
-      RSTG_CUDA(cudaMemcpyAsync(in_frames.p, frames, (size_t)B * n_top * 3 * esz,
-                                host_in ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
-      tune(f64, B);
-    }
+    if (!tuned && opts.autotune) tune(frames, f64, host_in, F);
     RSTG_CUDA(cudaMemsetAsync(diag.p, 0, 64, st));
     last_stats[0] = 0;
     for (int64_t f0 = 0; f0 < F; f0 += batch) {

@@ -85,7 +85,7 @@ struct System {
                     rstg_residue_energy* d_decomp, Prof* prof = nullptr);
   void launch_pairs(int variant, int64_t F);
   void launch_sasa(int warps, int64_t F);
-  void tune(bool f64, int64_t B);
+  void tune(const void* frames, bool f64, bool host_in, int64_t F);
 
  public:
   void profile(const float* d_frames, int64_t F, int32_t* n, char* names, double* ms, double* flops, double* bytes);

@@ -186,3 +186,13 @@ def test_cfg5_gb_frame(inputs):
     _binding_terms(out, fx["gb_accurate"])
     plain = _gb_system(rst, s, prm, "plain").run(fr)
     _plain_vs_faithful(plain, fx["gb_faithful"], 1e-10)
+
+
+@pytest.mark.gpu
+def test_cfg3_plain_pb_relative_frame(inputs):
+    rst = _rst()
+    s, fr, prm, fx = inputs(3)
+    plain = _pb_system(rst, s, prm, 3, mode="plain")
+    plain.set_pb_convergence(PB_REL_TOL)
+    out = plain.run(fr[:1])
+    _binding_terms(out, np.asarray(fx["pb_converged"])[:1], cols=(1, 4, 7, 10))
