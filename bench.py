@@ -212,7 +212,7 @@ def _polar_err(a, b):
     return {k: float(np.abs(np.asarray(a)[:n, c] - np.asarray(b)[:n, c]).max()) for k, c in POLAR}
 
 
-def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs, rel_tols=(1e-6, 1e-7)):
+def pbsa_leg(rst, ctx, n_frames, n_plain, peak_gbs, rel_tols=(1e-6, 1e-9)):
     """MM-PBSA on the 3,040-atom workload: frames/s of the batched engine on
     the reference's stopping rule and on the relative-residual rule (FP32
     V-cycles of a consistent multigrid under FP64 defect correction), beside
@@ -408,7 +408,7 @@ def serving_stream(rst, ctx, n_req, n_systems=32, seed=4, load=0.7):
             "arrival_mean_ms": 1e3 * mean_gap, "load": load}
 
 
-def large_mixed(rst, ctx, n_frames=500, per_request=50, pb_rel_tol=1e-7, seed=5):
+def large_mixed(rst, ctx, n_frames=500, per_request=50, pb_rel_tol=1e-9, seed=5):
     """25,000 + 80 atoms: MM-GBSA (SASA 960 points) and MM-PBSA (0.5 A grids of
     ~193^3, DH boundary, relative-residual stop) requests of per_request
     frames each, n_frames of each kind, interleaved in one serving loop with
