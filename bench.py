@@ -651,7 +651,7 @@ def main():
                            "frames_per_gpu": F, "l2": "256 MB flush between timed steps",
                            "parallelism": f"replicas x{world} (frames sharded, no exchange)"},
                 "gpu_launches": launches, "clocks": clk.summary(),
-                "precision_stats": stats}
+                "precision_stats": stats, "tuning": sysf.tuning()}
         line.update(extras)
         print(json.dumps(line), flush=True)
     if pg:
