@@ -346,6 +346,78 @@ struct PairOut {
   double gbC, gbR, gbL, dgb, mmR, mmL;
 };
 
+// The columns [lo, hi) of one 32-column mask word for one row: pair sums
+// into a[] (FP32), FP64 Lennard-Jones / Coulomb pairs marked in dfr.  kCls
+// is the tile's class, uniform over a block: 0 receptor x receptor or ligand
+// x ligand without exclusion / 1-4 masks, 1 the same with masks, 2 receptor x
+// ligand (only the complex GB pair energy: the cross pairs' Lennard-Jones,
+// Coulomb and binding GB terms are summed in FP64 by k_rl_rows), 3 a tile
+// that straddles the receptor / ligand boundary (pair by pair).
+struct PairRow {
+  float4 xi, Ri;
+  float dRi, iRc, iRs;
+  int ti;
+  bool in_r;
+};
+
+template <int kCls>
+__device__ __forceinline__ void pair_word(int lo, int hi, int j0, int nR, const PairRow& P, int nt, const GbConstF& k,
+                                          const float4* __restrict__ sx, const float4* __restrict__ sR,
+                                          const float* __restrict__ sdR, const int* __restrict__ st,
+                                          const float2* __restrict__ slj, unsigned wex, unsigned w14, float (&a)[6],
+                                          unsigned& dfr) {
+#pragma unroll 2
+  for (int jj = lo; jj < hi; jj++) {
+    const float4 xj = sx[jj];
+    const float dx = P.xi.x - xj.x, dy = P.xi.y - xj.y, dz = P.xi.z - xj.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    if (r2 > k.fcut2) continue;
+    const float4 Rj = sR[jj];
+    const float qq = P.xi.w * xj.w;
+    const bool same = kCls == 2 ? false : (kCls == 3 ? ((j0 + jj < nR) == P.in_r) : true);
+    const float tc = 0.25f * r2 * P.iRc * Rj.z;
+    const float RRc = P.Ri.x * Rj.x;
+    float eC, f2C, finvC, EC;
+    const float pC = gb_pair_parts(qq, r2, RRc, tc, k, eC, f2C, finvC, EC);
+    a[0] += pC;
+    if (kCls == 2 || !same) continue;
+    const float ts = 0.25f * r2 * P.iRs * Rj.w;
+    const float dRR = fmaf(P.Ri.x, sdR[jj], Rj.y * P.dRi);  // RcRc' - RsRs'
+    const float dp = (dRR == 0.f || (tc >= 16.f && ts >= 16.f))
+                         ? 0.f
+                         : gb_pair_delta(qq, r2, RRc, P.Ri.y * Rj.y, P.iRs * Rj.w, dRR, tc, ts, eC, f2C, finvC, EC, k);
+    a[P.in_r ? 1 : 2] += pC - dp;
+    a[3] += dp;
+    const int b = jj & 31;
+    const bool is14 = kCls == 0 ? false : ((w14 >> b) & 1u), excl = kCls == 0 ? false : ((wex >> b) & 1u);
+    if (is14 || (!excl && r2 < kNbGuard2)) {
+      dfr |= 1u << b;
+    } else if (!excl) {
+      const float2 ab = slj[P.ti * nt + st[jj]];
+      const float rinv = rsqrtf(r2), ir2 = rinv * rinv, ir6 = ir2 * ir2 * ir2;
+      a[P.in_r ? 4 : 5] += fmaf(ab.x * ir6, ir6, fmaf(-ab.y, ir6, qq * rinv));
+    }
+  }
+}
+
+template <int kCls, int kWords>
+__device__ __forceinline__ void pair_row(int cb, int jstart, int m, int j0, int nR, const PairRow& P, int nt,
+                                         const GbConstF& k, const float4* sx, const float4* sR, const float* sdR,
+                                         const int* st, const float2* slj, const unsigned (&mex)[kWords],
+                                         const unsigned (&m14)[kWords], unsigned (&defer)[kWords], double (&acc)[6]) {
+#pragma unroll
+  for (int w = 0; w < kWords; w++) {
+    const int lo = max(cb + 32 * w, jstart), hi = min(cb + 32 * w + 32, m);
+    if (lo >= hi) continue;
+    float a[6] = {0, 0, 0, 0, 0, 0};
+    unsigned dfr = 0u;
+    pair_word<kCls>(lo, hi, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex[w], m14[w], a, dfr);
+    defer[w] = dfr;
+#pragma unroll
+    for (int q = 0; q < 6; q++) acc[q] += (double)a[q];
+  }
+}
+
 // One 128 x 128 tile per block.  TPR threads share a row: thread
 // (row, part) takes the row's columns [part*128/TPR, (part+1)*128/TPR), so
 // TPR > 1 gives more, smaller threads per tile (TPR and the register cap
@@ -388,15 +460,21 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
     }
   }
   __syncthreads();
+  // tile class (uniform over the block)
+  const bool rowR = (bi + 1) * kTile <= nR, rowL = bi * kTile >= nR;
+  const bool colR = (bj + 1) * kTile <= nR, colL = bj * kTile >= nR;
+  const int cls = ((rowR && colR) || (rowL && colL)) ? (rec >= 0 ? 1 : 0) : (((rowR && colL) || (rowL && colR)) ? 2 : 3);
   double acc[6] = {0, 0, 0, 0, 0, 0};
   int n64 = 0;
   if (i < nC) {
-    float4 xi = X[i];
-    float4 Ri = RF[i];
-    float dRi = DR[i];
-    int ti = type[i];
-    bool in_r = i < nR;
-    float iRc = Ri.z, iRs = Ri.w;
+    PairRow P;
+    P.xi = X[i];
+    P.Ri = RF[i];
+    P.dRi = DR[i];
+    P.ti = type[i];
+    P.in_r = i < nR;
+    P.iRc = P.Ri.z;
+    P.iRs = P.Ri.w;
     const int cb = cpart * kCols;  // first column of this thread
     unsigned mex[kWords], m14[kWords], defer[kWords];
 #pragma unroll
@@ -409,55 +487,20 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
         m14[w] = mr[kTile * 4 + w];
       }
     }
-    int m = min(cb + kCols, nC - j0);
-    int jstart = (bi == bj) ? max(row + 1, cb) : cb;
-    // one 32-column word of the masks per step (unrolled: the mask words stay in registers)
-#pragma unroll
-    for (int w = 0; w < kWords; w++) {
-      const int lo = max(cb + 32 * w, jstart), hi = min(cb + 32 * w + 32, m);
-      if (lo >= hi) continue;
-      const unsigned wex = mex[w], w14 = m14[w];
-      unsigned dfr = 0u;
-      float a[6] = {0, 0, 0, 0, 0, 0};
-      for (int jj = lo; jj < hi; jj++) {
-        int j = j0 + jj;
-        float4 xj = sx[jj];
-        float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        if (r2 > k.fcut2) continue;
-        float4 Rj = sR[jj];
-        float qq = xi.w * xj.w;
-        bool same = (j < nR) == in_r;
-        float iRcj = Rj.z;
-        float tc = 0.25f * r2 * iRc * iRcj;
-        float RRc = Ri.x * Rj.x;
-        float eC, f2C, finvC, EC;
-        float pC = gb_pair_parts(qq, r2, RRc, tc, k, eC, f2C, finvC, EC);
-        a[0] += pC;
-        if (same) {
-          float iRsj = Rj.w;
-          float ts = 0.25f * r2 * iRs * iRsj;
-          float dRR = fmaf(Ri.x, sdR[jj], Rj.y * dRi);  // RcRc' - RsRs'
-          float iRRs = iRs * iRsj;
-          float dp = (dRR == 0.f || (tc >= 16.f && ts >= 16.f))
-                         ? 0.f
-                         : gb_pair_delta(qq, r2, RRc, Ri.y * Rj.y, iRRs, dRR, tc, ts, eC, f2C, finvC, EC, k);
-          a[in_r ? 1 : 2] += pC - dp;
-          a[3] += dp;
-          const int b = jj & 31;
-          const bool is14 = (w14 >> b) & 1u, excl = (wex >> b) & 1u;
-          if (is14 || (!excl && r2 < kNbGuard2)) {
-            dfr |= 1u << b;
-          } else if (!excl) {
-            float2 ab = slj[ti * nt + st[jj]];
-            float rinv = rsqrtf(r2), ir2 = rinv * rinv, ir6 = ir2 * ir2 * ir2;
-            a[in_r ? 4 : 5] += fmaf(ab.x * ir6, ir6, fmaf(-ab.y, ir6, qq * rinv));
-          }
-        }  // receptor x ligand GB pairs enter the binding difference in FP64 (k_rl_rows)
-      }
-      defer[w] = dfr;
-#pragma unroll
-      for (int q = 0; q < 6; q++) acc[q] += (double)a[q];
+    const int m = min(cb + kCols, nC - j0);
+    const int jstart = (bi == bj) ? max(row + 1, cb) : cb;
+    switch (cls) {
+      case 0:
+        pair_row<0, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
+        break;
+      case 1:
+        pair_row<1, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
+        break;
+      case 2:
+        pair_row<2, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
+        break;
+      default:
+        pair_row<3, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
     }
     // deferred FP64 Lennard-Jones / Coulomb pairs of this thread
     double e64 = 0.0;
@@ -468,13 +511,13 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
         const int b = __ffs(mk) - 1;
         mk &= mk - 1;
         const int jj = cb + 32 * w + b, j = j0 + jj;
-        const int cls = ((m14[w] >> b) & 1u) ? 2 : 1;
-        const double2 ab = lj64[ti * nt + st[jj]];
-        e64 += nb64(X64, i, j, (double)xi.w * (double)sx[jj].w, ab.x, ab.y, cls, scee, scnb);
+        const int c14 = ((m14[w] >> b) & 1u) ? 2 : 1;
+        const double2 ab = lj64[P.ti * nt + st[jj]];
+        e64 += nb64(X64, i, j, (double)P.xi.w * (double)sx[jj].w, ab.x, ab.y, c14, scee, scnb);
         n64++;
       }
     }
-    acc[in_r ? 4 : 5] += e64;
+    acc[P.in_r ? 4 : 5] += e64;
   }
   if (n64) atomicAdd((unsigned long long*)(diag + 4), (unsigned long long)n64);
   double* p = part + ((long long)f * gridDim.x + blockIdx.x) * 6;
