@@ -320,16 +320,18 @@ rstg_status rstg_system_run_device(rstg_system* s, const float* d_frames, int64_
  * re-checked in FP64, [3] neighbour-list overflows (must be 0). */
 rstg_status rstg_system_last_stats(const rstg_system* s, int64_t* stats4);
 
-/* Launch shapes of a fused system (no reference counterpart).  shape8 =
+/* Launch shapes of a fused system (no reference counterpart).  shape12 =
  * pair-kernel threads per tile row, its minimum resident blocks per SM
  * (register cap), SASA warps per block, frames per batch, tuned (1 once the
  * first run timed the candidates), frames of the tuning pass, number of
- * pair-kernel candidates, number of SASA candidates; ms8 = the tuning pass's
- * best-of-two milliseconds per candidate (pair-kernel shapes first, then
- * SASA shapes).  Systems of one process with the same device, atom counts
- * and sphere points share the tuned shapes, so equal inputs give equal
- * results.  Either pointer may be NULL; zeros for plain-mode systems. */
-rstg_status rstg_system_tuning(const rstg_system* s, int32_t* shape8, double* ms8);
+ * pair-kernel candidates, number of SASA candidates, Born-radius kernel
+ * threads per row, its minimum resident blocks per SM, number of its
+ * candidates, 0; ms12 = the tuning pass's best-of-two milliseconds per
+ * candidate (pair-kernel shapes, then SASA shapes, then Born-radius shapes).
+ * Systems of one process with the same device, atom counts and sphere
+ * points share the tuned shapes, so equal inputs give equal results.  Either
+ * pointer may be NULL; zeros for plain-mode systems. */
+rstg_status rstg_system_tuning(const rstg_system* s, int32_t* shape12, double* ms12);
 
 /* Batched Poisson-Boltzmann engine of a fused PB system (no reference
  * counterpart), accumulated over runs: grids solved, lock-step multigrid

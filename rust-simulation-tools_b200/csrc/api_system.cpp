@@ -190,15 +190,15 @@ rstg_status rstg_system_last_stats(const rstg_system* s, int64_t* st) {
   });
 }
 
-rstg_status rstg_system_tuning(const rstg_system* s, int32_t* shape8, double* ms8) {
+rstg_status rstg_system_tuning(const rstg_system* s, int32_t* shape12, double* ms12) {
   return guard([&] {
     if (!s) throw Error(RSTG_ERR_INVALID, "system must not be NULL");
     if (s->opts.mode != RSTG_MODE_FUSED || !s->fp) {
-      if (shape8) memset(shape8, 0, 8 * sizeof(int32_t));
-      if (ms8) memset(ms8, 0, 8 * sizeof(double));
+      if (shape12) memset(shape12, 0, 12 * sizeof(int32_t));
+      if (ms12) memset(ms12, 0, 12 * sizeof(double));
       return;
     }
-    s->tuning(shape8, ms8);
+    s->tuning(shape12, ms12);
   });
 }
 

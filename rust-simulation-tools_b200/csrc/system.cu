@@ -153,19 +153,29 @@ __device__ __forceinline__ float hct_far(float x, float rinv) {
   return x * x2 * rinv * p;
 }
 
-__global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __restrict__ xyz32,
-                                               const double* __restrict__ xyz64, const float4* __restrict__ P32,
-                                               const double* __restrict__ rho64, const double* __restrict__ sj64,
-                                               const double* __restrict__ rad64, const double* __restrict__ q64,
-                                               GbConstF k, float probe, int cap, int* __restrict__ nbr,
-                                               int* __restrict__ nbrcnt, double* __restrict__ R64,
-                                               float4* __restrict__ Rf, float* __restrict__ dRf,
-                                               double* __restrict__ part,
-                                               int* __restrict__ diag) {
+// One block per 128 rows (atoms i) of a frame, all columns j in 128-wide
+// shared-memory tiles.  TPR threads share a row, each taking a fixed share
+// of every tile's columns (TPR and the register cap MINB are picked per
+// system by the tuner); the row's shares are added in a fixed order, and its
+// SASA neighbour list is filled through a shared-memory counter (entry order
+// does not matter: k_sasa orders the list itself and a point's burial does
+// not depend on the order of its tests).
+template <int TPR, int MINB>
+__global__ void __launch_bounds__(kTile * TPR, MINB)
+    k_psi(int nC, int nR, const float4* __restrict__ xyz32, const double* __restrict__ xyz64,
+          const float4* __restrict__ P32, const double* __restrict__ rho64, const double* __restrict__ sj64,
+          const double* __restrict__ rad64, const double* __restrict__ q64, GbConstF k, float probe, int cap,
+          int* __restrict__ nbr, int* __restrict__ nbrcnt, double* __restrict__ R64, float4* __restrict__ Rf,
+          float* __restrict__ dRf, double* __restrict__ part, int* __restrict__ diag) {
+  constexpr int kCols = kTile / TPR, kWords = kCols / 32;
+  static_assert(kCols % 32 == 0, "columns per thread in whole words");
   __shared__ float4 sx[kTile];
   __shared__ float2 sp[kTile];
   __shared__ double sh[32];
-  int f = blockIdx.y, i = blockIdx.x * kTile + threadIdx.x;
+  __shared__ int scnt[kTile];
+  __shared__ double2 spsi[TPR > 1 ? kTile * (TPR - 1) : 1];
+  const int row = threadIdx.x % kTile, cpart = threadIdx.x / kTile, cb = cpart * kCols;
+  int f = blockIdx.y, i = blockIdx.x * kTile + row;
   bool valid = i < nC;
   const float4* X = xyz32 + (long long)f * nC;
   const double* X64 = xyz64 + (long long)f * nC * 3;
@@ -175,53 +185,66 @@ __global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __r
   double rho_i64 = valid ? rho64[i] : 0.0;
   bool in_r = i < nR;
   double psi_own = 0.0, psi_oth = 0.0;
-  int cnt = 0, near64 = 0;
+  int near64 = 0;
+  if (cpart == 0) scnt[row] = 0;
   int* my = nbr + ((long long)f * nC + (valid ? i : 0)) * cap;
   for (int j0 = 0; j0 < nC; j0 += kTile) {
-    int jl = j0 + threadIdx.x;
-    if (jl < nC) {
-      sx[threadIdx.x] = X[jl];
-      float4 pj = P32[jl];
-      sp[threadIdx.x] = make_float2(pj.z, pj.w);
+    if (threadIdx.x < kTile) {
+      int jl = j0 + threadIdx.x;
+      if (jl < nC) {
+        sx[threadIdx.x] = X[jl];
+        float4 pj = P32[jl];
+        sp[threadIdx.x] = make_float2(pj.z, pj.w);
+      }
     }
     __syncthreads();
-    int m = min(kTile, nC - j0);
+    int m = min(cb + kCols, nC - j0);
     float po = 0.f, pc = 0.f;
-    unsigned nearm[kTile / 32] = {0, 0, 0, 0};  // tile columns that take the FP64 near path
+    unsigned nearm[kWords];  // tile columns that take the FP64 near path
+#pragma unroll
+    for (int w = 0; w < kWords; w++) nearm[w] = 0u;
     if (valid) {
-      for (int jj = 0; jj < m; jj++) {
-        int j = j0 + jj;
-        float4 xj = sx[jj];
-        float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        float2 s = sp[jj];
-        float ee = ext_i + s.y;
-        if (j != i && r2 <= fmaf(ee * ee, 1.00001f, 1e-4f)) {
-          if (cnt < cap) my[cnt] = j;
-          cnt++;
+#pragma unroll
+      for (int w = 0; w < kWords; w++) {  // one mask word per step: the word stays in a register
+        const int lo = cb + 32 * w, hi = min(lo + 32, m);
+        unsigned nw = 0u;
+#pragma unroll 2
+        for (int jj = lo; jj < hi; jj++) {
+          int j = j0 + jj;
+          float4 xj = sx[jj];
+          float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+          float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          float2 s = sp[jj];
+          float ee = ext_i + s.y;
+          if (j != i && r2 <= fmaf(ee * ee, 1.00001f, 1e-4f)) {
+            int c = TPR > 1 ? atomicAdd(&scnt[row], 1) : scnt[row]++;
+            if (c < cap) my[c] = j;
+          }
+          if (j == i || r2 > k.fcut2) continue;
+          float rinv = rsqrtf(r2), r = r2 * rinv, sj = s.x;
+          bool own = (j < nR) == in_r;
+          if (r2 > 0.f && 16.f * sj * sj <= r2 && rho_i <= r - sj) {
+            float t = hct_far(sj * rinv, rinv);
+            if (own)
+              po += t;
+            else
+              pc += t;
+          } else {
+            nw |= 1u << (jj & 31);
+          }
         }
-        if (j == i || r2 > k.fcut2) continue;
-        float rinv = rsqrtf(r2), r = r2 * rinv, sj = s.x;
-        bool own = (j < nR) == in_r;
-        if (r2 > 0.f && 16.f * sj * sj <= r2 && rho_i <= r - sj) {
-          float t = hct_far(sj * rinv, rinv);
-          if (own)
-            po += t;
-          else
-            pc += t;
-        } else {
-          nearm[jj >> 5] |= 1u << (jj & 31);
-        }
+        nearm[w] = nw;
       }
-      // near pairs of this tile, each thread over its own set (a warp runs as
-      // many FP64 evaluations as its busiest lane, not one per column any
-      // lane needs)
-      for (int w = 0; w < kTile / 32; w++) {
+      // near pairs of this tile, each thread over its own set (a warp runs
+      // as many FP64 evaluations as its busiest lane, not one per column
+      // any lane needs)
+#pragma unroll
+      for (int w = 0; w < kWords; w++) {
         unsigned mk = nearm[w];
         while (mk) {
           int b = __ffs(mk) - 1;
           mk &= mk - 1;
-          int j = j0 + 32 * w + b;
+          int j = j0 + cb + 32 * w + b;
           near64++;
           double ddx = X64[3 * i] - X64[3 * j], ddy = X64[3 * i + 1] - X64[3 * j + 1],
                  ddz = X64[3 * i + 2] - X64[3 * j + 2];
@@ -242,8 +265,20 @@ __global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __r
     psi_oth += (double)pc;
     __syncthreads();
   }
+  // the row's shares in a fixed order
+  if (TPR > 1) {
+    if (cpart > 0) spsi[(cpart - 1) * kTile + row] = make_double2(psi_own, psi_oth);
+    __syncthreads();
+    if (cpart == 0)
+      for (int q = 1; q < TPR; q++) {
+        double2 v = spsi[(q - 1) * kTile + row];
+        psi_own += v.x;
+        psi_oth += v.y;
+      }
+  }
   double sC = 0.0, sR = 0.0, sL = 0.0, sD = 0.0;
-  if (valid) {
+  if (valid && cpart == 0) {
+    int cnt = scnt[row];
     nbrcnt[(long long)f * nC + i] = cnt;
     if (cnt > cap) atomicMax(diag + 3, cnt);
     double Rc = radius64(psi_own + psi_oth, rho_i64, rad64[i], k.model, k.rgbmax);
@@ -274,6 +309,17 @@ __global__ void __launch_bounds__(kTile) k_psi(int nC, int nR, const float4* __r
     p[3] = sD;
   }
 }
+
+// Launch shapes of k_psi the tuner chooses from.
+using PsiFn = void (*)(int, int, const float4*, const double*, const float4*, const double*, const double*,
+                       const double*, const double*, GbConstF, float, int, int*, int*, double*, float4*, float*,
+                       double*, int*);
+struct PsiVariant {
+  int tpr, minb;
+  PsiFn fn;
+};
+static const PsiVariant kPsiVariants[] = {{1, 1, k_psi<1, 1>}, {1, 8, k_psi<1, 8>}, {2, 4, k_psi<2, 4>}};
+constexpr int kNumPsiVariants = (int)(sizeof(kPsiVariants) / sizeof(kPsiVariants[0]));
 
 // ---------------------------------------------------------------------------
 // K2: pair energies on triangular tiles
@@ -1314,6 +1360,16 @@ void System::launch_pairs(int variant, int64_t F) {
       split.complex.scee, split.complex.scnb, k2part.as<double>(), diag.as<int>());
 }
 
+void System::launch_psi(int variant, int64_t F) {
+  FusedParams& P = *fp;
+  const PsiVariant& v = kPsiVariants[variant];
+  int nb1 = (int)((nC + kTile - 1) / kTile);
+  v.fn<<<dim3((unsigned)nb1, (unsigned)F), kTile * v.tpr, 0, stream()>>>(
+      (int)nC, (int)nR, xyz32.as<float4>(), xyz64.as<double>(), P.P32.as<float4>(), P.rho64.as<double>(),
+      P.sj64.as<double>(), P.rad64.as<double>(), P.q64.as<double>(), P.gb, (float)P.probe, nbr_cap, nbr.as<int>(),
+      nbrcnt.as<int>(), R64.as<double>(), Rf.as<float4>(), dRf.as<float>(), k1part.as<double>(), diag.as<int>());
+}
+
 void System::launch_sasa(int warps, int64_t F) {
   FusedParams& P = *fp;
   size_t sm = sasa_smem(nbr_cap, warps);
@@ -1333,7 +1389,7 @@ struct TuneKey {
   }
 };
 static std::mutex g_tune_mu;
-static std::map<TuneKey, std::pair<int, int>> g_tuned;
+static std::map<TuneKey, std::tuple<int, int, int>> g_tuned;
 
 // Times every launch shape of k_pairs and k_sasa on the first frames of the
 // first run and keeps the fastest of each: best of two CUDA-event timed
@@ -1347,8 +1403,7 @@ void System::tune(const void* frames, bool f64, bool host_in, int64_t F) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) {
-      pairs_variant = it->second.first;
-      sasa_warps = it->second.second;
+      std::tie(psi_variant, pairs_variant, sasa_warps) = it->second;
       tuned = true;
       return;
     }
@@ -1383,6 +1438,17 @@ void System::tune(const void* frames, bool f64, bool host_in, int64_t F) {
     return best;
   };
   try {
+    float bq = 1e30f;
+    for (int v = 0; v < kNumPsiVariants; v++) {
+      float t = time_it([&] { launch_psi(v, TB); });
+      tune_ms[kNumPairsVariants + kNumSasaChoices + v] = t;
+      if (t < bq) {
+        bq = t;
+        psi_variant = v;
+      }
+    }
+    launch_psi(psi_variant, TB);  // the chosen shape's outputs feed the kernels timed next
+    launched(ctx, 1);
     float bp = 1e30f;
     for (int v = 0; v < kNumPairsVariants; v++) {
       tune_ms[v] = time_it([&] { launch_pairs(v, TB); });
@@ -1411,16 +1477,17 @@ void System::tune(const void* frames, bool f64, bool host_in, int64_t F) {
   tune_frames = TB;
   tuned = true;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tuned.emplace(key, std::make_pair(pairs_variant, sasa_warps));
+  g_tuned.emplace(key, std::make_tuple(psi_variant, pairs_variant, sasa_warps));
 }
 
-void System::tuning(int32_t* shape8, double* ms8) const {
+void System::tuning(int32_t* shape12, double* ms12) const {
   const PairsVariant& v = kPairsVariants[pairs_variant];
-  int32_t o[8] = {v.tpr, v.minb, sasa_warps, (int32_t)batch, tuned ? 1 : 0, (int32_t)tune_frames,
-                  kNumPairsVariants, kNumSasaChoices};
-  if (shape8) memcpy(shape8, o, sizeof(o));
-  if (ms8)
-    for (int k = 0; k < 8; k++) ms8[k] = tune_ms[k];
+  const PsiVariant& q = kPsiVariants[psi_variant];
+  int32_t o[12] = {v.tpr, v.minb, sasa_warps, (int32_t)batch, tuned ? 1 : 0, (int32_t)tune_frames,
+                   kNumPairsVariants, kNumSasaChoices, q.tpr, q.minb, kNumPsiVariants, 0};
+  if (shape12) memcpy(shape12, o, sizeof(o));
+  if (ms12)
+    for (int k = 0; k < 12; k++) ms12[k] = tune_ms[k];
 }
 
 void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_energy* d_out,
@@ -1450,12 +1517,7 @@ void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_
                                                                  P.slot_src.as<int>(), P.P32.as<float4>(),
                                                                  xyz64.as<double>(), xyz32.as<float4>());
   mark("prep", 0.0, Fd * (n_top * 12.0 + nCd * 40.0));
-  k_psi<<<dim3((unsigned)nb1, Fu), kTile, 0, st>>>((int)nC, (int)nR, xyz32.as<float4>(), xyz64.as<double>(),
-                                                   P.P32.as<float4>(), P.rho64.as<double>(), P.sj64.as<double>(),
-                                                   P.rad64.as<double>(), P.q64.as<double>(), P.gb,
-                                                   (float)P.probe, nbr_cap, nbr.as<int>(), nbrcnt.as<int>(),
-                                                   R64.as<double>(), Rf.as<float4>(), dRf.as<float>(), k1part.as<double>(),
-                                                   diag.as<int>());
+  launch_psi(psi_variant, F);
   mark("psi", Fd * nCd * (nCd - 1) * 32.0, 0.0);
   launch_pairs(pairs_variant, F);
   mark("pairs", Fd * (nCd * (nCd - 1) / 2 * gbf + same_pairs * (gbf + 22.0)), 0.0);

@@ -36,11 +36,12 @@ struct System {
   int nbr_cap = 320;
   // launch shapes (picked by tune() on the first run when opts.autotune)
   int pairs_variant = 0;  // index into the k_pairs shape table (system.cu)
+  int psi_variant = 0;    // index into the k_psi shape table
   int sasa_warps = 4;     // warps (atoms) per k_sasa block
   bool tuned = false;
   int64_t tune_frames = 0;
-  double tune_ms[8] = {};  // candidate times of the tuning run (k_pairs shapes, then k_sasa shapes)
-  void tuning(int32_t* shape8, double* ms8) const;
+  double tune_ms[12] = {};  // candidate times of the tuning run (k_pairs, k_sasa, k_psi shapes)
+  void tuning(int32_t* shape12, double* ms12) const;
 
   // per-batch buffers (fused)
   DevBuf in_frames, xyz64, xyz32, R64, Rf, dRf, nbr, nbrcnt, sasa, k1part, k2part, rows, cols, bpart, res_buf, dec_buf,
@@ -84,6 +85,7 @@ struct System {
   void launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_energy* d_out,
                     rstg_residue_energy* d_decomp, Prof* prof = nullptr);
   void launch_pairs(int variant, int64_t F);
+  void launch_psi(int variant, int64_t F);
   void launch_sasa(int warps, int64_t F);
   void tune(const void* frames, bool f64, bool host_in, int64_t F);
 

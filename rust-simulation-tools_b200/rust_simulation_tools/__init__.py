@@ -771,13 +771,15 @@ class BindingSystem:
     def tuning(self) -> dict:
         """Launch shapes of the fused engine (picked on the first run when
         autotuning) and the tuning pass's candidate times in ms."""
-        sh = (C.c_int32 * 8)()
-        ms = np.zeros(8)
+        sh = (C.c_int32 * 12)()
+        ms = np.zeros(12)
         check(N.lib.rstg_system_tuning(self._h, sh, _dp(ms)))
-        npair, nsasa = sh[6], sh[7]
+        npair, nsasa, npsi = sh[6], sh[7], sh[10]
         return {"pairs_threads_per_row": sh[0], "pairs_min_blocks_per_sm": sh[1], "sasa_warps_per_block": sh[2],
                 "batch_frames": sh[3], "tuned": bool(sh[4]), "tuning_frames": sh[5],
-                "pairs_candidates_ms": ms[:npair].tolist(), "sasa_candidates_ms": ms[npair:npair + nsasa].tolist()}
+                "psi_threads_per_row": sh[8], "psi_min_blocks_per_sm": sh[9],
+                "pairs_candidates_ms": ms[:npair].tolist(), "sasa_candidates_ms": ms[npair:npair + nsasa].tolist(),
+                "psi_candidates_ms": ms[npair + nsasa:npair + nsasa + npsi].tolist()}
 
     def pb_stats(self) -> dict:
         """Batched PB engine totals of a fused PB system (zeros otherwise)."""
