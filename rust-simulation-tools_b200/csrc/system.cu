@@ -464,120 +464,137 @@ __device__ __forceinline__ void pair_row(int cb, int jstart, int m, int j0, int 
   }
 }
 
-// One 128 x 128 tile per block.  TPR threads share a row: thread
-// (row, part) takes the row's columns [part*128/TPR, (part+1)*128/TPR), so
-// TPR > 1 gives more, smaller threads per tile (TPR and the register cap
-// MINB are picked per system by the tuner).  Pairs whose Lennard-Jones /
-// Coulomb term takes the FP64 path (closer than 3.5 A, or 1-4) are marked in
-// a per-thread bit mask and evaluated after the column loop, each thread over
-// its own marks, so a warp runs as many FP64 evaluations as its busiest lane
-// rather than one for every column where any lane needs one.
+// Persistent blocks over work items (tile, frame): the Lennard-Jones type
+// table is staged in shared memory once per block, then each item is one
+// 128 x 128 tile of one frame.  TPR threads share a row: thread (row, part)
+// takes the row's columns [part*128/TPR, (part+1)*128/TPR), so TPR > 1 gives
+// more, smaller threads per tile (TPR and the register cap MINB are picked
+// per system by the tuner).  Pairs whose Lennard-Jones / Coulomb term takes
+// the FP64 path (closer than 3.5 A, or 1-4) are marked in a per-thread bit
+// mask and evaluated after the column loop, each thread over its own marks,
+// so a warp runs as many FP64 evaluations as its busiest lane rather than
+// one for every column where any lane needs one.  Each item's six sums are
+// reduced in a fixed order and written to its own slot.
 template <int TPR, int MINB>
 __global__ void __launch_bounds__(kTile * TPR, MINB)
-    k_pairs(int nC, int nR, const int4* __restrict__ tiles, const float4* __restrict__ xyz32,
-            const double* __restrict__ xyz64, const float4* __restrict__ Rf, const float* __restrict__ dRf,
-            const int* __restrict__ type, int nt, const float2* __restrict__ lj32, const double2* __restrict__ lj64,
-            const unsigned* __restrict__ masks, GbConstF k, double scee, double scnb, double* __restrict__ part,
-            int* __restrict__ diag) {
-  constexpr int kCols = kTile / TPR, kWords = kCols / 32;
+    k_pairs(int nC, int nR, const int4* __restrict__ tiles, int ntiles, long long nitems,
+            const float4* __restrict__ xyz32, const double* __restrict__ xyz64, const float4* __restrict__ Rf,
+            const float* __restrict__ dRf, const int* __restrict__ type, int nt, const float2* __restrict__ lj32,
+            const double2* __restrict__ lj64, const unsigned* __restrict__ masks, GbConstF k, double scee,
+            double scnb, double* __restrict__ part, int* __restrict__ diag) {
+  constexpr int kCols = kTile / TPR, kWords = kCols / 32, kWarps = kTile * TPR / 32;
   static_assert(kCols % 32 == 0, "columns per thread in whole words");
   extern __shared__ float2 slj[];  // nt*nt (A, B)
   __shared__ float4 sx[kTile];
   __shared__ float4 sR[kTile];
   __shared__ float sdR[kTile];
   __shared__ int st[kTile];
-  __shared__ double sh[32];
+  __shared__ double sh[6][kWarps];
   for (int t = threadIdx.x; t < nt * nt; t += blockDim.x) slj[t] = lj32[t];
-  int4 tl = tiles[blockIdx.x];
-  int f = blockIdx.y, bi = tl.x, bj = tl.y, rec = tl.z;
   const int row = threadIdx.x % kTile, cpart = threadIdx.x / kTile;
-  int i = bi * kTile + row, j0 = bj * kTile;
-  const float4* X = xyz32 + (long long)f * nC;
-  const double* X64 = xyz64 + (long long)f * nC * 3;
-  const float4* RF = Rf + (long long)f * nC;
-  const float* DR = dRf + (long long)f * nC;
-  if (threadIdx.x < kTile) {
-    int jl = j0 + threadIdx.x;
-    if (jl < nC) {
-      sx[threadIdx.x] = X[jl];
-      sR[threadIdx.x] = RF[jl];
-      sdR[threadIdx.x] = DR[jl];
-      st[threadIdx.x] = type[jl];
-    }
-  }
-  __syncthreads();
-  // tile class (uniform over the block)
-  const bool rowR = (bi + 1) * kTile <= nR, rowL = bi * kTile >= nR;
-  const bool colR = (bj + 1) * kTile <= nR, colL = bj * kTile >= nR;
-  const int cls = ((rowR && colR) || (rowL && colL)) ? (rec >= 0 ? 1 : 0) : (((rowR && colL) || (rowL && colR)) ? 2 : 3);
-  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int n64 = 0;
-  if (i < nC) {
-    PairRow P;
-    P.xi = X[i];
-    P.Ri = RF[i];
-    P.dRi = DR[i];
-    P.ti = type[i];
-    P.in_r = i < nR;
-    P.iRc = P.Ri.z;
-    P.iRs = P.Ri.w;
-    const int cb = cpart * kCols;  // first column of this thread
-    unsigned mex[kWords], m14[kWords], defer[kWords];
+  for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int f = (int)(item / ntiles), ti_ = (int)(item % ntiles);
+    const int4 tl = tiles[ti_];
+    const int bi = tl.x, bj = tl.y, rec = tl.z;
+    const int i = bi * kTile + row, j0 = bj * kTile;
+    const float4* X = xyz32 + (long long)f * nC;
+    const double* X64 = xyz64 + (long long)f * nC * 3;
+    const float4* RF = Rf + (long long)f * nC;
+    const float* DR = dRf + (long long)f * nC;
+    __syncthreads();  // the previous item's readers of the column tile are done
+    if (threadIdx.x < kTile) {
+      int jl = j0 + threadIdx.x;
+      if (jl < nC) {
+        sx[threadIdx.x] = X[jl];
+        sR[threadIdx.x] = RF[jl];
+        sdR[threadIdx.x] = DR[jl];
+        st[threadIdx.x] = type[jl];
+      }
+    }
+    __syncthreads();
+    // tile class (uniform over the block)
+    const bool rowR = (bi + 1) * kTile <= nR, rowL = bi * kTile >= nR;
+    const bool colR = (bj + 1) * kTile <= nR, colL = bj * kTile >= nR;
+    const int cls =
+        ((rowR && colR) || (rowL && colL)) ? (rec >= 0 ? 1 : 0) : (((rowR && colL) || (rowL && colR)) ? 2 : 3);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    if (i < nC) {
+      PairRow P;
+      P.xi = X[i];
+      P.Ri = RF[i];
+      P.dRi = DR[i];
+      P.ti = type[i];
+      P.in_r = i < nR;
+      P.iRc = P.Ri.z;
+      P.iRs = P.Ri.w;
+      const int cb = cpart * kCols;  // first column of this thread
+      unsigned mex[kWords], m14[kWords], defer[kWords];
 #pragma unroll
-    for (int w = 0; w < kWords; w++) mex[w] = m14[w] = defer[w] = 0u;
-    if (rec >= 0) {
-      const unsigned* mr = masks + ((long long)rec * 2 * kTile + row) * 4 + cb / 32;
+      for (int w = 0; w < kWords; w++) mex[w] = m14[w] = defer[w] = 0u;
+      if (rec >= 0) {
+        const unsigned* mr = masks + ((long long)rec * 2 * kTile + row) * 4 + cb / 32;
+#pragma unroll
+        for (int w = 0; w < kWords; w++) {
+          mex[w] = mr[w];
+          m14[w] = mr[kTile * 4 + w];
+        }
+      }
+      const int m = min(cb + kCols, nC - j0);
+      const int jstart = (bi == bj) ? max(row + 1, cb) : cb;
+      switch (cls) {
+        case 0:
+          pair_row<0, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
+          break;
+        case 1:
+          pair_row<1, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
+          break;
+        case 2:
+          pair_row<2, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
+          break;
+        default:
+          pair_row<3, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
+      }
+      // deferred FP64 Lennard-Jones / Coulomb pairs of this thread
+      double e64 = 0.0;
 #pragma unroll
       for (int w = 0; w < kWords; w++) {
-        mex[w] = mr[w];
-        m14[w] = mr[kTile * 4 + w];
+        unsigned mk = defer[w];
+        while (mk) {
+          const int b = __ffs(mk) - 1;
+          mk &= mk - 1;
+          const int jj = cb + 32 * w + b, j = j0 + jj;
+          const int c14 = ((m14[w] >> b) & 1u) ? 2 : 1;
+          const double2 ab = lj64[P.ti * nt + st[jj]];
+          e64 += nb64(X64, i, j, (double)P.xi.w * (double)sx[jj].w, ab.x, ab.y, c14, scee, scnb);
+          n64++;
+        }
       }
+      acc[P.in_r ? 4 : 5] += e64;
     }
-    const int m = min(cb + kCols, nC - j0);
-    const int jstart = (bi == bj) ? max(row + 1, cb) : cb;
-    switch (cls) {
-      case 0:
-        pair_row<0, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
-        break;
-      case 1:
-        pair_row<1, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
-        break;
-      case 2:
-        pair_row<2, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
-        break;
-      default:
-        pair_row<3, kWords>(cb, jstart, m, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex, m14, defer, acc);
-    }
-    // deferred FP64 Lennard-Jones / Coulomb pairs of this thread
-    double e64 = 0.0;
+    // the item's six sums: warps, then the warp sums in order (one barrier)
 #pragma unroll
-    for (int w = 0; w < kWords; w++) {
-      unsigned mk = defer[w];
-      while (mk) {
-        const int b = __ffs(mk) - 1;
-        mk &= mk - 1;
-        const int jj = cb + 32 * w + b, j = j0 + jj;
-        const int c14 = ((m14[w] >> b) & 1u) ? 2 : 1;
-        const double2 ab = lj64[P.ti * nt + st[jj]];
-        e64 += nb64(X64, i, j, (double)P.xi.w * (double)sx[jj].w, ab.x, ab.y, c14, scee, scnb);
-        n64++;
-      }
+    for (int q = 0; q < 6; q++) {
+      const double v = warp_sum(acc[q]);
+      if (lane == 0) sh[q][warp] = v;
     }
-    acc[P.in_r ? 4 : 5] += e64;
+    __syncthreads();
+    if (threadIdx.x < 6) {
+      double v = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarps; w++) v += sh[threadIdx.x][w];
+      part[(long long)item * 6 + threadIdx.x] = v;
+    }
   }
   if (n64) atomicAdd((unsigned long long*)(diag + 4), (unsigned long long)n64);
-  double* p = part + ((long long)f * gridDim.x + blockIdx.x) * 6;
-  for (int q = 0; q < 6; q++) {
-    double v = block_sum(acc[q], sh);
-    if (threadIdx.x == 0) p[q] = v;
-  }
 }
 
 // Launch shapes of k_pairs the tuner chooses from: threads per row (TPR) and
 // the minimum resident blocks per SM that caps registers per thread.
-using PairsFn = void (*)(int, int, const int4*, const float4*, const double*, const float4*, const float*,
-                         const int*, int, const float2*, const double2*, const unsigned*, GbConstF, double, double,
-                         double*, int*);
+using PairsFn = void (*)(int, int, const int4*, int, long long, const float4*, const double*, const float4*,
+                         const float*, const int*, int, const float2*, const double2*, const unsigned*, GbConstF,
+                         double, double, double*, int*);
 struct PairsVariant {
   int tpr, minb;
   PairsFn fn;
@@ -1354,10 +1371,15 @@ void System::launch_pairs(int variant, int64_t F) {
   FusedParams& P = *fp;
   const PairsVariant& v = kPairsVariants[variant];
   size_t ljsm = (size_t)P.nt * P.nt * sizeof(float2);
-  v.fn<<<dim3((unsigned)P.ntiles, (unsigned)F), kTile * v.tpr, ljsm, stream()>>>(
-      (int)nC, (int)nR, P.tiles.as<int4>(), xyz32.as<float4>(), xyz64.as<double>(), Rf.as<float4>(), dRf.as<float>(),
-      P.type.as<int>(), P.nt, P.lj32.as<float2>(), P.lj64.as<double2>(), P.masks.as<unsigned>(), P.gb,
-      split.complex.scee, split.complex.scnb, k2part.as<double>(), diag.as<int>());
+  // persistent grid: the resident blocks of the shape, a whole number of SMs
+  int& per_sm = pairs_per_sm[variant];
+  if (per_sm == 0) RSTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, kTile * v.tpr, ljsm));
+  long long items = (long long)P.ntiles * F;
+  long long grid = std::min<long long>(items, (long long)std::max(per_sm, 1) * ctx->prop.multiProcessorCount);
+  v.fn<<<(unsigned)grid, kTile * v.tpr, ljsm, stream()>>>(
+      (int)nC, (int)nR, P.tiles.as<int4>(), P.ntiles, items, xyz32.as<float4>(), xyz64.as<double>(), Rf.as<float4>(),
+      dRf.as<float>(), P.type.as<int>(), P.nt, P.lj32.as<float2>(), P.lj64.as<double2>(), P.masks.as<unsigned>(),
+      P.gb, split.complex.scee, split.complex.scnb, k2part.as<double>(), diag.as<int>());
 }
 
 void System::launch_psi(int variant, int64_t F) {

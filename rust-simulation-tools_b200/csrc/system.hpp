@@ -37,6 +37,7 @@ struct System {
   // launch shapes (picked by tune() on the first run when opts.autotune)
   int pairs_variant = 0;  // index into the k_pairs shape table (system.cu)
   int psi_variant = 0;    // index into the k_psi shape table
+  int pairs_per_sm[8] = {};  // resident k_pairs blocks per SM of each shape (persistent grid), 0 until queried
   int sasa_warps = 4;     // warps (atoms) per k_sasa block
   bool tuned = false;
   int64_t tune_frames = 0;
