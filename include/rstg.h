@@ -204,7 +204,6 @@ rstg_status rstg_mm_energy_compute(rstg_ctx* ctx, const rstg_topology* t, const 
 /* compute_gb_energy, crates/mmpbsa/src/gb_energy.rs:357-365 */
 rstg_status rstg_gb_energy_compute(rstg_ctx* ctx, const rstg_topology* t, const double* xyz, int64_t n,
                                    const rstg_gb_params* p, double* total, double* born_radii);
-/* compute_sa_energy, crates/mmpbsa/src/sa_energy.rs:51-75 */
 /* Born-radius cache across frames (gb_energy.rs:66-120): when the RMSD
  * between the coordinates and the cached ones is below rmsd_threshold (A),
  * compute_gb_energy_cached (gb_energy.rs:372-387) reuses the cached radii;
@@ -216,6 +215,7 @@ void rstg_gb_cache_destroy(rstg_gb_cache* c);
 rstg_status rstg_gb_energy_cached(rstg_ctx* ctx, const rstg_topology* t, const double* xyz, int64_t n,
                                   const rstg_gb_params* p, rstg_gb_cache* cache, double* total, double* born_radii,
                                   int32_t* reused);
+/* compute_sa_energy, crates/mmpbsa/src/sa_energy.rs:51-75 */
 rstg_status rstg_sa_energy_compute(rstg_ctx* ctx, const rstg_topology* t, const double* xyz, int64_t n,
                                    const rstg_sa_params* p, double* total, double* total_sasa, double* per_atom);
 /* compute_pb_energy / compute_pb_energy_solvated, crates/mmpbsa/src/pb_energy.rs:332-482;

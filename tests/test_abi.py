@@ -133,3 +133,31 @@ def test_compute_without_gpu_raises(small_system):
     top = rst.read_prmtop(prm)
     with pytest.raises(Exception):
         rst.compute_gb_energy(top, fr[0] / 10.0)
+
+
+def test_rust_binding_declares_every_entry_point():
+    """The Rust binding a crate maintainer drops in declares every function
+    of include/rstg.h, and each #[repr(C)] struct has the header's fields in
+    the header's order."""
+    import re
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    h = open(os.path.join(root, "include", "rstg.h")).read()
+    r = open(os.path.join(root, "rust-simulation-tools_b200", "bindings", "rstg_sys.rs")).read()
+    names = set(re.findall(r"\b(rstg_[a-z0-9_]+)\s*\(", h))
+    assert names and all(("fn " + n + "(") in r for n in names), sorted(n for n in names if ("fn " + n + "(") not in r)
+    for st in ("rstg_gb_params", "rstg_pb_params", "rstg_frame_energy", "rstg_topology_desc", "rstg_system_opts",
+               "rstg_server_opts", "rstg_pb_diag"):
+        body = re.search(r"typedef struct " + st + r" \{(.*?)\} " + st + ";", h, re.S).group(1)
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        fields = []
+        for decl in body.split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            for part in decl.split(","):
+                nm = re.findall(r"([A-Za-z_][A-Za-z0-9_]*)\s*(?:\[[^\]]*\])?\s*$", part.strip())
+                if nm:
+                    fields.append(nm[0])
+        rs = re.search(r"pub struct " + st + r" \{(.*?)\n\}", r, re.S).group(1)
+        assert re.findall(r"pub ([a-z_0-9]+):", rs) == fields, st
