@@ -326,7 +326,9 @@ rstg_status rstg_system_last_stats(const rstg_system* s, int64_t* stats4);
  * first run timed the candidates), frames of the tuning pass, number of
  * pair-kernel candidates, number of SASA candidates, Born-radius kernel
  * threads per row, its minimum resident blocks per SM, number of its
- * candidates, 0; ms12 = the tuning pass's best-of-two milliseconds per
+ * candidates, pair-kernel form (0 one block per 128 x 128 tile with
+ * threads-per-row threads per row, 1 warp items with the tile's columns in
+ * threads-per-row shares); ms12 = the tuning pass's best-of-two milliseconds per
  * candidate (pair-kernel shapes, then SASA shapes, then Born-radius shapes).
  * Systems of one process with the same device, atom counts and sphere
  * points share the tuned shapes, so equal inputs give equal results.  Either

@@ -406,14 +406,17 @@ struct PairRow {
   bool in_r;
 };
 
+// Columns come from shared memory (k_pairs) or, read at one address per
+// warp, from global memory (k_pairs_w); lanes skip columns before `first`.
 template <int kCls>
-__device__ __forceinline__ void pair_word(int lo, int hi, int j0, int nR, const PairRow& P, int nt, const GbConstF& k,
-                                          const float4* __restrict__ sx, const float4* __restrict__ sR,
-                                          const float* __restrict__ sdR, const int* __restrict__ st,
-                                          const float2* __restrict__ slj, unsigned wex, unsigned w14, float (&a)[6],
-                                          unsigned& dfr) {
+__device__ __forceinline__ void pair_word(int lo, int hi, int first, int j0, int nR, const PairRow& P, int nt,
+                                          const GbConstF& k, const float4* __restrict__ sx,
+                                          const float4* __restrict__ sR, const float* __restrict__ sdR,
+                                          const int* __restrict__ st, const float2* __restrict__ slj, unsigned wex,
+                                          unsigned w14, float (&a)[6], unsigned& dfr) {
 #pragma unroll 2
   for (int jj = lo; jj < hi; jj++) {
+    if (jj < first) continue;
     const float4 xj = sx[jj];
     const float dx = P.xi.x - xj.x, dy = P.xi.y - xj.y, dz = P.xi.z - xj.z;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -457,7 +460,7 @@ __device__ __forceinline__ void pair_row(int cb, int jstart, int m, int j0, int 
     if (lo >= hi) continue;
     float a[6] = {0, 0, 0, 0, 0, 0};
     unsigned dfr = 0u;
-    pair_word<kCls>(lo, hi, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex[w], m14[w], a, dfr);
+    pair_word<kCls>(lo, hi, lo, j0, nR, P, nt, k, sx, sR, sdR, st, slj, mex[w], m14[w], a, dfr);
     defer[w] = dfr;
 #pragma unroll
     for (int q = 0; q < 6; q++) acc[q] += (double)a[q];
@@ -590,17 +593,138 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
   if (n64) atomicAdd((unsigned long long*)(diag + 4), (unsigned long long)n64);
 }
 
+// Warp-item form of k_pairs: every warp takes its own work items (frame,
+// tile, 32-row group, 1/H of the tile's columns) with no block-wide barrier
+// after the type table is staged; the column data are read at one address
+// per warp from global memory (L1 hits after the first row group).  Each
+// item's six sums are reduced over the warp in a fixed order into the item's
+// own slot: items are ordered frame, tile, row group, column share, so a
+// frame's items are contiguous for k_reduce.
+template <int H, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    k_pairs_w(int nC, int nR, const int4* __restrict__ tiles, int ntiles, long long nitems,
+              const float4* __restrict__ xyz32, const double* __restrict__ xyz64, const float4* __restrict__ Rf,
+              const float* __restrict__ dRf, const int* __restrict__ type, int nt, const float2* __restrict__ lj32,
+              const double2* __restrict__ lj64, const unsigned* __restrict__ masks, GbConstF k, double scee,
+              double scnb, double* __restrict__ part, int* __restrict__ diag) {
+  constexpr int kCols = kTile / H, kWords = kCols / 32, kSub = 4 * H;
+  extern __shared__ float2 slj[];  // nt*nt (A, B)
+  for (int t = threadIdx.x; t < nt * nt; t += blockDim.x) slj[t] = lj32[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  int n64 = 0;
+  for (long long item = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < nitems;
+       item += nwarps) {
+    const long long per_frame = (long long)ntiles * kSub;
+    const int f = (int)(item / per_frame);
+    const int r = (int)(item % per_frame), ti_ = r / kSub, g = (r % kSub) / H, h = r % H;
+    const int4 tl = tiles[ti_];
+    const int bi = tl.x, bj = tl.y, rec = tl.z;
+    const int row = 32 * g + lane, i = bi * kTile + row, j0 = bj * kTile;
+    const float4* X = xyz32 + (long long)f * nC;
+    const double* X64 = xyz64 + (long long)f * nC * 3;
+    const float4* RF = Rf + (long long)f * nC;
+    const float* DR = dRf + (long long)f * nC;
+    const bool rowR = (bi + 1) * kTile <= nR, rowL = bi * kTile >= nR;
+    const bool colR = (bj + 1) * kTile <= nR, colL = bj * kTile >= nR;
+    const int cls =
+        ((rowR && colR) || (rowL && colL)) ? (rec >= 0 ? 1 : 0) : (((rowR && colL) || (rowL && colR)) ? 2 : 3);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const int cb = h * kCols;
+    const int m = min(cb + kCols, nC - j0);
+    // warp-uniform start (diagonal tiles: the group's first row + 1), per-lane first column
+    const int wstart = (bi == bj) ? max(32 * g + 1, cb) : cb;
+    const int first = (bi == bj) ? max(row + 1, cb) : cb;
+    const bool live = i < nC && wstart < m;
+    PairRow P;
+    unsigned mex[kWords], m14[kWords], defer[kWords];
+#pragma unroll
+    for (int w = 0; w < kWords; w++) mex[w] = m14[w] = defer[w] = 0u;
+    if (live) {
+      P.xi = X[i];
+      P.Ri = RF[i];
+      P.dRi = DR[i];
+      P.ti = type[i];
+      P.in_r = i < nR;
+      P.iRc = P.Ri.z;
+      P.iRs = P.Ri.w;
+      if (rec >= 0) {
+        const unsigned* mr = masks + ((long long)rec * 2 * kTile + row) * 4 + cb / 32;
+#pragma unroll
+        for (int w = 0; w < kWords; w++) {
+          mex[w] = mr[w];
+          m14[w] = mr[kTile * 4 + w];
+        }
+      }
+      const float4* cx = X + j0;
+      const float4* cR = RF + j0;
+      const float* cd = DR + j0;
+      const int* ct = type + j0;
+#pragma unroll
+      for (int w = 0; w < kWords; w++) {
+        const int lo = max(cb + 32 * w, wstart), hi = min(cb + 32 * w + 32, m);
+        if (lo >= hi) continue;
+        float a[6] = {0, 0, 0, 0, 0, 0};
+        unsigned dfr = 0u;
+        switch (cls) {
+          case 0:
+            pair_word<0>(lo, hi, first, j0, nR, P, nt, k, cx, cR, cd, ct, slj, mex[w], m14[w], a, dfr);
+            break;
+          case 1:
+            pair_word<1>(lo, hi, first, j0, nR, P, nt, k, cx, cR, cd, ct, slj, mex[w], m14[w], a, dfr);
+            break;
+          case 2:
+            pair_word<2>(lo, hi, first, j0, nR, P, nt, k, cx, cR, cd, ct, slj, mex[w], m14[w], a, dfr);
+            break;
+          default:
+            pair_word<3>(lo, hi, first, j0, nR, P, nt, k, cx, cR, cd, ct, slj, mex[w], m14[w], a, dfr);
+        }
+        defer[w] = dfr;
+#pragma unroll
+        for (int q = 0; q < 6; q++) acc[q] += (double)a[q];
+      }
+      double e64 = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWords; w++) {
+        unsigned mk = defer[w];
+        while (mk) {
+          const int b = __ffs(mk) - 1;
+          mk &= mk - 1;
+          const int jj = cb + 32 * w + b, j = j0 + jj;
+          const int c14 = ((m14[w] >> b) & 1u) ? 2 : 1;
+          const double2 ab = lj64[P.ti * nt + ct[jj]];
+          e64 += nb64(X64, i, j, (double)P.xi.w * (double)cx[jj].w, ab.x, ab.y, c14, scee, scnb);
+          n64++;
+        }
+      }
+      acc[P.in_r ? 4 : 5] += e64;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const double v = warp_sum(acc[q]);
+      if (lane == q) part[item * 6 + q] = v;
+    }
+  }
+  if (n64) atomicAdd((unsigned long long*)(diag + 4), (unsigned long long)n64);
+}
+
 // Launch shapes of k_pairs the tuner chooses from: threads per row (TPR) and
 // the minimum resident blocks per SM that caps registers per thread.
 using PairsFn = void (*)(int, int, const int4*, int, long long, const float4*, const double*, const float4*,
                          const float*, const int*, int, const float2*, const double2*, const unsigned*, GbConstF,
                          double, double, double*, int*);
+// warp: 0 block-tile kernel (tpr threads per row, sums per (frame, tile)),
+// 1 warp-item kernel (tpr = H column shares, sums per (frame, tile, row
+// group, share)); sub = items per (frame, tile).
 struct PairsVariant {
-  int tpr, minb;
+  int warp, tpr, minb, sub;
   PairsFn fn;
 };
-static const PairsVariant kPairsVariants[] = {
-    {1, 6, k_pairs<1, 6>}, {1, 4, k_pairs<1, 4>}, {2, 3, k_pairs<2, 3>}, {2, 4, k_pairs<2, 4>}, {4, 2, k_pairs<4, 2>}};
+static const PairsVariant kPairsVariants[] = {{0, 1, 6, 1, k_pairs<1, 6>}, {0, 2, 4, 1, k_pairs<2, 4>},
+                                              {1, 1, 4, 4, k_pairs_w<1, 4>}, {1, 2, 4, 8, k_pairs_w<2, 4>},
+                                              {1, 1, 3, 4, k_pairs_w<1, 3>}, {1, 2, 3, 8, k_pairs_w<2, 3>}};
+constexpr int kMaxPairsSub = 8;
 constexpr int kNumPairsVariants = (int)(sizeof(kPairsVariants) / sizeof(kPairsVariants[0]));
 static const int kSasaWarpChoices[] = {4, 2, 8};
 constexpr int kNumSasaChoices = 3;
@@ -1346,7 +1470,7 @@ void System::ensure_buffers(int64_t frames) {
   nbrcnt = DevBuf(B * nC * 4, st);
   sasa = DevBuf(B * nC * 16, st);
   k1part = DevBuf(B * nb1 * 4 * 8, st);
-  k2part = DevBuf(B * (int64_t)fp->ntiles * 6 * 8, st);
+  k2part = DevBuf(B * (int64_t)fp->ntiles * kMaxPairsSub * 6 * 8, st);
   rows = DevBuf(B * std::max<int64_t>(nR, 1) * 24, st);
   cols = DevBuf(B * std::max<int64_t>(nL, 1) * 16, st);
   bpart = DevBuf(B * nbp * 5 * 8, st);
@@ -1373,10 +1497,14 @@ void System::launch_pairs(int variant, int64_t F) {
   size_t ljsm = (size_t)P.nt * P.nt * sizeof(float2);
   // persistent grid: the resident blocks of the shape, a whole number of SMs
   int& per_sm = pairs_per_sm[variant];
-  if (per_sm == 0) RSTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, kTile * v.tpr, ljsm));
-  long long items = (long long)P.ntiles * F;
-  long long grid = std::min<long long>(items, (long long)std::max(per_sm, 1) * ctx->prop.multiProcessorCount);
-  v.fn<<<(unsigned)grid, kTile * v.tpr, ljsm, stream()>>>(
+  if (per_sm == 0)
+    RSTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warp ? 256 : kTile * v.tpr, ljsm));
+  const int threads = v.warp ? 256 : kTile * v.tpr;
+  long long items = (long long)P.ntiles * v.sub * F;
+  long long per_block = v.warp ? threads / 32 : 1;
+  long long grid = std::min<long long>((items + per_block - 1) / per_block,
+                                       (long long)std::max(per_sm, 1) * ctx->prop.multiProcessorCount);
+  v.fn<<<(unsigned)grid, threads, ljsm, stream()>>>(
       (int)nC, (int)nR, P.tiles.as<int4>(), P.ntiles, items, xyz32.as<float4>(), xyz64.as<double>(), Rf.as<float4>(),
       dRf.as<float>(), P.type.as<int>(), P.nt, P.lj32.as<float2>(), P.lj64.as<double2>(), P.masks.as<unsigned>(),
       P.gb, split.complex.scee, split.complex.scnb, k2part.as<double>(), diag.as<int>());
@@ -1506,7 +1634,7 @@ void System::tuning(int32_t* shape12, double* ms12) const {
   const PairsVariant& v = kPairsVariants[pairs_variant];
   const PsiVariant& q = kPsiVariants[psi_variant];
   int32_t o[12] = {v.tpr, v.minb, sasa_warps, (int32_t)batch, tuned ? 1 : 0, (int32_t)tune_frames,
-                   kNumPairsVariants, kNumSasaChoices, q.tpr, q.minb, kNumPsiVariants, 0};
+                   kNumPairsVariants, kNumSasaChoices, q.tpr, q.minb, kNumPsiVariants, v.warp};
   if (shape12) memcpy(shape12, o, sizeof(o));
   if (ms12)
     for (int k = 0; k < 12; k++) ms12[k] = tune_ms[k];
@@ -1572,7 +1700,8 @@ void System::launch_batch(const void* d_frames, bool f64, int64_t F, rstg_frame_
     RSTG_CUDA(cudaMemsetAsync(bpart.p, 0, bpart.bytes, st));
   }
   double f0 = -0.5 * (1.0 / solv.gb.solute_dielectric - 1.0 / solv.gb.solvent_dielectric);
-  k_reduce<<<Fu, 256, 0, st>>>((int)nC, (int)nR, nb1, P.ntiles, nbp, k1part.as<double>(), k2part.as<double>(),
+  k_reduce<<<Fu, 256, 0, st>>>((int)nC, (int)nR, nb1, P.ntiles * kPairsVariants[pairs_variant].sub, nbp,
+                               k1part.as<double>(), k2part.as<double>(),
                                sasa.as<double>(), rows.as<double>(), cols.as<double>(), bpart.as<double>(),
                                R64.as<double>(), P.q64.as<double>(), sa.surface_tension, sa.offset, f0, P.nres,
                                P.res_ptr.as<int>(), P.res_slots.as<int>(), d_out, d_decomp);

@@ -778,6 +778,7 @@ class BindingSystem:
         return {"pairs_threads_per_row": sh[0], "pairs_min_blocks_per_sm": sh[1], "sasa_warps_per_block": sh[2],
                 "batch_frames": sh[3], "tuned": bool(sh[4]), "tuning_frames": sh[5],
                 "psi_threads_per_row": sh[8], "psi_min_blocks_per_sm": sh[9],
+                "pairs_form": "warp items" if sh[11] else "block per tile",
                 "pairs_candidates_ms": ms[:npair].tolist(), "sasa_candidates_ms": ms[npair:npair + nsasa].tolist(),
                 "psi_candidates_ms": ms[npair + nsasa:npair + nsasa + npsi].tolist()}
 
