@@ -60,7 +60,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <memory>
+#include <thread>
 
 #include "common.cuh"
 #include "pb_batch.hpp"
@@ -1128,6 +1130,12 @@ void PbBatchEngine::release() {
 PbBatchEngine::~PbBatchEngine() {
   if (graph_) cudaGraphExecDestroy(graph_);
   for (cudaEvent_t e : prof_events_) cudaEventDestroy(e);
+  for (cudaEvent_t e : setup_events_) cudaEventDestroy(e);
+  if (start_event_) cudaEventDestroy(start_event_);
+  for (cudaStream_t w : setup_streams_) {
+    cudaStreamSynchronize(w);
+    cudaStreamDestroy(w);
+  }
 }
 
 void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, const std::vector<double*>* phi_out) {
@@ -1202,18 +1210,56 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   RSTG_CUDA(cudaMemsetAsync(P32, 0, b32, st));
 
   // ---- maps and boundary values (FP64, the reference's set-up) -------------
-  for (int j = 0; j < nj; j++) {
-    PbJob& J = jobs[j];
-    size_t n = J.g.n();
-    double* base = P64 + lay[j].o64;
-    const F64Lay f = f64_lay(J);
-    double *phi = base, *rho = J.rho_of >= 0 ? nullptr : base + f.rho * n;
-    double* m = base + f.maps * n;
-    double *ex = J.uniform ? nullptr : m, *ey = J.uniform ? nullptr : m + n, *ez = J.uniform ? nullptr : m + 2 * n,
-           *k2 = J.uniform ? nullptr : m + 3 * n;
-    pb_maps_into(c_, J.g, *J.atoms, p, J.ein, J.eout, J.kap, J.ionic, rho, ex, ey, ez, k2);
-    RSTG_CUDA(cudaMemsetAsync(phi, 0, n * 8, st));
-    if (J.bc.kind != 1) pb_boundary(c_, J.g, phi, *J.atoms, J.bc);
+  // One grid's set-up is a chain of small launches with host waits (the
+  // exterior flood fill tests for its fixed point every eight passes), so the
+  // grids are spread over worker threads, each on its own stream; the main
+  // stream waits for all of them before the cycles start.
+  {
+    const int W = (int)std::min<size_t>(kSetupWorkers, (size_t)nj);
+    int dev = 0;
+    RSTG_CUDA(cudaGetDevice(&dev));
+    while ((int)setup_streams_.size() < W) {
+      cudaStream_t w;
+      RSTG_CUDA(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking));
+      setup_streams_.push_back(w);
+      cudaEvent_t e;
+      RSTG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      setup_events_.push_back(e);
+    }
+    if (!start_event_) RSTG_CUDA(cudaEventCreateWithFlags(&start_event_, cudaEventDisableTiming));
+    RSTG_CUDA(cudaEventRecord(start_event_, st));  // the pools are allocated and cleared on st
+    std::vector<std::exception_ptr> err(W);
+    auto work = [&](int w) {
+      try {
+        cudaSetDevice(dev);
+        cudaStream_t ws = setup_streams_[w];
+        RSTG_CUDA(cudaStreamWaitEvent(ws, start_event_, 0));
+        PbStreamScope sc(ws);
+        for (int j = w; j < nj; j += W) {
+          PbJob& J = jobs[j];
+          size_t n = J.g.n();
+          double* base = P64 + lay[j].o64;
+          const F64Lay f = f64_lay(J);
+          double *phi = base, *rho = J.rho_of >= 0 ? nullptr : base + f.rho * n;
+          double* m = base + f.maps * n;
+          double *ex = J.uniform ? nullptr : m, *ey = J.uniform ? nullptr : m + n,
+                 *ez = J.uniform ? nullptr : m + 2 * n, *k2 = J.uniform ? nullptr : m + 3 * n;
+          pb_maps_into(c_, J.g, *J.atoms, p, J.ein, J.eout, J.kap, J.ionic, rho, ex, ey, ez, k2);
+          RSTG_CUDA(cudaMemsetAsync(phi, 0, n * 8, ws));
+          if (J.bc.kind != 1) pb_boundary(c_, J.g, phi, *J.atoms, J.bc);
+        }
+        RSTG_CUDA(cudaEventRecord(setup_events_[w], ws));
+      } catch (...) {
+        err[w] = std::current_exception();
+      }
+    };
+    std::vector<std::thread> th;
+    for (int w = 1; w < W; w++) th.emplace_back(work, w);
+    work(0);
+    for (auto& t : th) t.join();
+    for (auto& e : err)
+      if (e) std::rethrow_exception(e);
+    for (int w = 0; w < W; w++) RSTG_CUDA(cudaStreamWaitEvent(st, setup_events_[w], 0));
   }
   std::vector<double*> phi_now(nj);  // current potential buffer of each grid (host view)
   for (int j = 0; j < nj; j++) phi_now[j] = P64 + lay[j].o64;

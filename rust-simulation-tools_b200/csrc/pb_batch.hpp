@@ -71,6 +71,10 @@ class PbBatchEngine {
   cudaStream_t st_;
   DevBuf pool64_, pool32_, pool8_, desc_, part_, small_, lists_;
   cudaGraphExec_t graph_ = nullptr;
+  static constexpr int kSetupWorkers = 8;       // threads (and streams) of the per-grid set-up
+  std::vector<cudaStream_t> setup_streams_;
+  std::vector<cudaEvent_t> setup_events_;
+  cudaEvent_t start_event_ = nullptr;
   std::vector<cudaEvent_t> prof_events_;
 };
 
