@@ -796,11 +796,15 @@ __global__ void k_coarse32(WL w, const LvlD* __restrict__ L, int lvl, const JobS
 // of 332.0522 q exp(-kappa r) / (eps_out r), pair terms in FP32 (coordinates
 // relative to the grid origin), accumulated in FP64.  Reference grids
 // (kappa = 0) skip the exponential.
+// phi2 (may be null): a second grid of the same geometry and atoms whose
+// boundary values take kappa kap2 and eout2 -- a solvated solve and its
+// reference solve share the distance work.
 struct DhD {
   double* phi;
+  double* phi2;
   const double *xyz, *q;
   int nx, ny, nz, na;
-  double ox, oy, oz, h, kap, eout;
+  double ox, oy, oz, h, kap, eout, kap2, eout2;
 };
 
 // Boundary points enumerated face by face: the two z faces, the two y faces
@@ -850,9 +854,9 @@ __global__ void __launch_bounds__(256) k_dh32(WL w, const DhD* __restrict__ D) {
   int ix = 0, iy = 0, iz = 0;
   bool valid = k < nb && bnd_point(d.nx, d.ny, d.nz, k, ix, iy, iz);
   float px = (float)(ix * d.h), py = (float)(iy * d.h), pz = (float)(iz * d.h);
-  float kap = (float)d.kap;
-  bool ionic = d.kap != 0.0;
-  double acc = 0.0;
+  const float kap = (float)d.kap, kap2 = (float)d.kap2;
+  const bool ionic = d.kap != 0.0, ionic2 = d.kap2 != 0.0, two = d.phi2 != nullptr;
+  double acc = 0.0, acc2 = 0.0;
   for (int a0 = 0; a0 < d.na; a0 += 256) {
     int a = a0 + threadIdx.x;
     if (a < d.na)
@@ -868,13 +872,18 @@ __global__ void __launch_bounds__(256) k_dh32(WL w, const DhD* __restrict__ D) {
         if (r2 <= 1e-20f) continue;
         float ir = rsqrtf(r2);
         float term = A.w * ir;
-        if (ionic) term *= __expf(-kap * (r2 * ir));
-        acc += (double)term;
+        const float r = r2 * ir;
+        acc += (double)(ionic ? term * __expf(-kap * r) : term);
+        if (two) acc2 += (double)(ionic2 ? term * __expf(-kap2 * r) : term);
       }
     }
     __syncthreads();
   }
-  if (valid) d.phi[ix + (long long)d.nx * (iy + (long long)d.ny * iz)] = 332.0522 * acc / d.eout;
+  if (valid) {
+    const long long o = ix + (long long)d.nx * (iy + (long long)d.ny * iz);
+    d.phi[o] = 332.0522 * acc / d.eout;
+    if (two) d.phi2[o] = 332.0522 * acc2 / d.eout2;
+  }
 }
 
 // Level-0 FP32 maps from the FP64 maps, then injection to coarser levels
@@ -1268,10 +1277,24 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     std::vector<DhD> dd;
     Lists dl;
     int sd = dl.add_slot();
+    std::vector<char> listed(nj, 0), merged(nj, 0);
+    for (int j : which) listed[j] = 1;
     for (int j : which) {
+      if (merged[j]) continue;
       const PbJob& J = jobs[j];
       DhD x;
       x.phi = phi_now[j];
+      x.phi2 = nullptr;
+      x.kap2 = 0.0;
+      x.eout2 = 1.0;
+      for (int k2 = j + 1; k2 < nj; k2++)  // the reference solve on the same grid and atoms
+        if (listed[k2] && !merged[k2] && jobs[k2].rho_of == j) {
+          x.phi2 = phi_now[k2];
+          x.kap2 = jobs[k2].bc.kappa;
+          x.eout2 = jobs[k2].bc.eout;
+          merged[k2] = 1;
+          break;
+        }
       x.xyz = J.atoms->xyz.as<double>();
       x.q = J.atoms->q.as<double>();
       x.nx = J.g.nx;
