@@ -138,7 +138,7 @@ struct Lv {
   float *__restrict__ e, *__restrict__ e2, *__restrict__ rhs, *__restrict__ res;
   const float *__restrict__ ex, *__restrict__ ey, *__restrict__ ez, *__restrict__ k2;
   const uint8_t* __restrict__ cd;
-  int nx, ny, nz, sy, sz, zc;
+  int nx, ny, nz, sy, sz, zc, hp;
   bool uni;
   float ih, om, w6, fin, fout, kb;
 };
@@ -159,6 +159,7 @@ __device__ __forceinline__ Lv lv_load(const LvlD* __restrict__ L, int j, int lvl
   v.nz = d.nz;
   v.sy = d.px;
   v.sz = d.px * d.ny;
+  v.hp = d.px >> 1;
   v.zc = d.zc;
   v.uni = d.uniform != 0;
   v.ih = d.ih;
@@ -176,6 +177,14 @@ __device__ __forceinline__ T face(unsigned c, const T* __restrict__ m, int i, T 
   return c == 0u ? eout : (c == 1u ? ein : m[i]);
 }
 
+// Split rows: every FP32 level array and the stencil codes store a row as its
+// even-x points followed, half a row pitch later, by its odd-x points, so the
+// points of one colour of a red-black sweep are contiguous in a row and move
+// as 16-byte vectors.  hp is the half pitch (elements).
+__device__ __forceinline__ int xo(int x, int hp) { return (x & 1) * hp + (x >> 1); }
+__device__ __forceinline__ int ixp(int i, int x, int hp) { return (x & 1) ? i - hp + 1 : i + hp; }  // x + 1
+__device__ __forceinline__ int ixm(int i, int x, int hp) { return (x & 1) ? i - hp : i + hp - 1; }  // x - 1
+
 // Brick of 32 x 8 x 8 points for a 256-thread block: thread (lane, warp) owns
 // the column (x, y) = (x0 + lane, y0 + warp) over the brick's 8 z planes, so
 // the index arithmetic is done once per block and the 8 points of a column
@@ -190,19 +199,19 @@ __device__ __forceinline__ void brick_col(int lb, int nx, int ny, int& x, int& y
 
 // FP32 7-point stencil of pb_solver.rs:250-317: ns = sum of eps-weighted
 // neighbours, dg = diagonal.
-__device__ __forceinline__ void st32(const Lv& d, const float* __restrict__ e, int i, float& ns, float& dg) {
-  const int sy = d.sy, sz = d.sz;
+__device__ __forceinline__ void st32(const Lv& d, const float* __restrict__ e, int x, int i, float& ns, float& dg) {
+  const int sy = d.sy, sz = d.sz, ip = ixp(i, x, d.hp), im = ixm(i, x, d.hp);
   if (d.uni) {
-    ns = d.w6 * ((e[i + 1] + e[i - 1]) + (e[i + sy] + e[i - sy]) + (e[i + sz] + e[i - sz]));
+    ns = d.w6 * ((e[ip] + e[im]) + (e[i + sy] + e[i - sy]) + (e[i + sz] + e[i - sz]));
     dg = 6.0f * d.w6;
   } else {
     const unsigned c0 = d.cd[i];
-    float a = face(c0 & 3u, d.ex, i, d.fin, d.fout), b = face(d.cd[i - 1] & 3u, d.ex, i - 1, d.fin, d.fout),
+    float a = face(c0 & 3u, d.ex, i, d.fin, d.fout), b = face(d.cd[im] & 3u, d.ex, im, d.fin, d.fout),
           c = face((c0 >> 2) & 3u, d.ey, i, d.fin, d.fout),
           dd = face((d.cd[i - sy] >> 2) & 3u, d.ey, i - sy, d.fin, d.fout),
           f = face((c0 >> 4) & 3u, d.ez, i, d.fin, d.fout),
           g = face((d.cd[i - sz] >> 4) & 3u, d.ez, i - sz, d.fin, d.fout);
-    ns = ((a * e[i + 1] + b * e[i - 1]) + (c * e[i + sy] + dd * e[i - sy]) + (f * e[i + sz] + g * e[i - sz])) * d.ih;
+    ns = ((a * e[ip] + b * e[im]) + (c * e[i + sy] + dd * e[i - sy]) + (f * e[i + sz] + g * e[i - sz])) * d.ih;
     dg = ((a + b) + (c + dd) + (f + g)) * d.ih + ((c0 & 64u) ? d.kb : 0.0f);
   }
 }
@@ -225,12 +234,13 @@ __global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__
   const double din = d.din, dout = d.dout, dkb = d.dkb;
   const bool uni = d.uniform != 0;
   const double ih = d.ih, wt = d.eps * d.ih;
-  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny, hp = d.px >> 1;
   int x, y, z0;
   brick_col(lb, nx, ny, x, y, z0);
   double acc = 0.0;
   if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
-    int i = x + sy * y + sz * z0, ci = x + cy * y + cz * z0;  // FP64 and padded FP32 / code indices
+    int i = x + sy * y + sz * z0, ci = xo(x, hp) + cy * y + cz * z0;  // FP64 and split FP32 / code indices
+    const int dxm = ixm(0, x, hp);                                     // code offset of x - 1
 #pragma unroll
     for (int k = 0; k < 8; k++, i += sz, ci += cz) {
       int z = z0 + k;
@@ -241,7 +251,7 @@ __global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__
         ns = wt * ((p[i + 1] + p[i - 1]) + (p[i + sy] + p[i - sy]) + (p[i + sz] + p[i - sz]));
         dg = 6.0 * wt;
       } else {
-        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci - 1] & 3u, ex, i - 1, din, dout),
+        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci + dxm] & 3u, ex, i - 1, din, dout),
                c = face((c0 >> 2) & 3u, ey, i, din, dout), dd = face((cd[ci - cy] >> 2) & 3u, ey, i - sy, din, dout),
                f = face((c0 >> 4) & 3u, ez, i, din, dout), g = face((cd[ci - cz] >> 4) & 3u, ez, i - sz, din, dout);
         ns = (a * p[i + 1] + b * p[i - 1]) * ih + (c * p[i + sy] + dd * p[i - sy]) * ih +
@@ -283,13 +293,14 @@ __global__ void __launch_bounds__(256, 4) k_upres64(WL w, const JobD* __restrict
   const double din = d.din, dout = d.dout, dkb = d.dkb;
   const bool uni = d.uniform != 0;
   const double ih = d.ih, wt = d.eps * d.ih;
-  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny, hp = d.px >> 1;
   int x, y, z0;
   brick_col(lb, nx, ny, x, y, z0);
   double acc = 0.0;
   if (x < nx && y < ny) {
     const bool inxy = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
-    int i = x + sy * y + sz * z0, ci = x + cy * y + cz * z0;  // FP64 and padded FP32 / code indices
+    int i = x + sy * y + sz * z0, ci = xo(x, hp) + cy * y + cz * z0;  // FP64 and split FP32 / code indices
+    const int dxp = ixp(0, x, hp), dxm = ixm(0, x, hp);              // offsets of x + 1, x - 1
 #pragma unroll 1
     for (int k = 0; k < 8; k++, i += sz, ci += cz) {
       const int z = z0 + k;
@@ -297,7 +308,7 @@ __global__ void __launch_bounds__(256, 4) k_upres64(WL w, const JobD* __restrict
       const double v = p[i] + (double)e0[ci];
       q[i] = v;
       if (!inxy || z < 1 || z > nz - 2) continue;
-      const double vxp = p[i + 1] + (double)e0[ci + 1], vxm = p[i - 1] + (double)e0[ci - 1],
+      const double vxp = p[i + 1] + (double)e0[ci + dxp], vxm = p[i - 1] + (double)e0[ci + dxm],
                    vyp = p[i + sy] + (double)e0[ci + cy], vym = p[i - sy] + (double)e0[ci - cy],
                    vzp = p[i + sz] + (double)e0[ci + cz], vzm = p[i - sz] + (double)e0[ci - cz];
       const unsigned c0 = cd[ci];
@@ -306,7 +317,7 @@ __global__ void __launch_bounds__(256, 4) k_upres64(WL w, const JobD* __restrict
         ns = wt * ((vxp + vxm) + (vyp + vym) + (vzp + vzm));
         dg = 6.0 * wt;
       } else {
-        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci - 1] & 3u, ex, i - 1, din, dout),
+        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci + dxm] & 3u, ex, i - 1, din, dout),
                c = face((c0 >> 2) & 3u, ey, i, din, dout), dd = face((cd[ci - cy] >> 2) & 3u, ey, i - sy, din, dout),
                f = face((c0 >> 4) & 3u, ez, i, din, dout), g = face((cd[ci - cz] >> 4) & 3u, ez, i - sz, din, dout);
         ns = (a * vxp + b * vxm) * ih + (c * vyp + dd * vym) * ih + (f * vzp + g * vzm) * ih;
@@ -367,8 +378,8 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
 // One full red-black sweep on one level (pb_solver.rs:250-317): every even
 // point (x + y + z even) from its odd neighbours, then every odd point from
 // the updated even ones, each point with the arithmetic of the
-// single-colour update.  A block owns an x-y tile of kSwTX x kSwTY points and
-// marches a chunk of z planes.  Planes of the correction (with a two-point
+// single-colour update.  A block owns an x-y tile of 32 x 16 points and
+// marches a chunk of z planes.  Planes of the correction (with a two-row
 // halo), of the right-hand side and of the stencil codes stream into
 // shared-memory rings with cp.async, two steps ahead of their use.  Step s
 // updates, in one phase between barriers, the even points of plane s+2 over
@@ -376,29 +387,32 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
 // neighbours in planes s-1 .. s+1 are already updated) and writes plane s-1
 // out.  Halo values are recomputed by each tile that needs them, so the sweep
 // reads `src` and writes the whole grid, boundary values copied, into `dst`:
-// no block reads what another block writes.  Each thread's points, copy
-// chunks and store are fixed for the whole march (only the colour parity
-// alternates with the plane), so the per-step index work is a few adds; a
-// half-warp covers 16 points of one colour in a row and the next half-warp
-// the next row (opposite parity), so the shared loads are free of bank
-// conflicts; ring depths are powers of two.
+// no block reads what another block writes.
+//
+// Rows are split by x parity in global and shared memory (see xo), so the
+// points of one colour in a row are contiguous: a thread updates four of
+// them with 16-byte loads of the point values, of each of the y / z
+// neighbour rows, of the right-hand side and of the other half (the x
+// neighbours), and 4-byte loads of four stencil codes.  160 threads: 64
+// update four odd points of plane s each (16 rows x 4 quads), 72 four even
+// points of plane s+2 (18 rows: the tile and a y halo row on each side), 18
+// the even point of the x halo of a row (x = xt-1 or xt+32, whichever is
+// even-coloured).
 // z planes per block: long marches on the finest level, short ones on the
 // coarse levels (few tiles per grid there, so more chunks keep the SMs busy)
-constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 288, kSwZC0 = 48, kSwZC1 = 16;
+constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 160, kSwZC0 = 48, kSwZC1 = 16;
 int sweep_chunk(int lvl) { return lvl == 0 ? kSwZC0 : (lvl == 1 ? kSwZC1 : 8); }
-constexpr int kSwW = kSwTX + 8;   // shared row: x in [xt-4, xt+TX+4), 16-byte chunks
+constexpr int kSwHW = 24;         // shared half-row: half-indices [hx0-4, hx0+20), hx0 = xt/2
+constexpr int kSwW = 2 * kSwHW;   // shared row: even half, then odd half
 constexpr int kSwEY = kSwTY + 4;  // correction rows: y in [yt-2, yt+TY+2)
 constexpr int kSwRY = kSwTY + 2;  // right-hand-side rows: y in [yt-1, yt+TY+1)
 constexpr int kSwCY = kSwTY + 3;  // code rows: y in [yt-2, yt+TY+1)
 constexpr int kSwNE = 8, kSwNR = 8, kSwNC = 8;  // ring depths in planes (slot = plane & (depth - 1))
-// first point of a thread: even points of plane s+2 inside the tile's x range, 16 per row, rows yt-1 .. yt+TY;
-// second point: odd points of plane s (threads < TY*16), then the even points of plane s+2 on the
-// x halo (one per row: x = xt-1 or xt+TX)
-static_assert(kSwTX == 32 && (kSwTY + 2) * 16 == kSwThreads && kSwTY * 16 + kSwTY + 2 <= kSwThreads,
-              "point assignment of the sweep");
-static_assert(kSwEY * (kSwW / 4) <= kSwThreads && kSwRY * (kSwW / 4) <= kSwThreads &&
-                  kSwCY * (kSwW / 4) <= kSwThreads && kSwTY * (kSwTX / 4) <= kSwThreads,
-              "one copy chunk and one store per thread and plane");
+constexpr int kSwChunks = kSwHW / 4;           // 16-byte (or 4-code) chunks per half-row
+static_assert(kSwTX == 32 && kSwTY == 16, "thread roles of the sweep");
+static_assert(kSwEY * 2 * kSwChunks <= 2 * kSwThreads && kSwRY * 2 * kSwChunks <= 2 * kSwThreads &&
+                  kSwCY * 2 * kSwChunks <= 2 * kSwThreads && kSwTY * 2 * 4 <= kSwThreads,
+              "two copy chunks and one store per thread and plane");
 
 struct SwSmem {
   float e[kSwNE][kSwEY * kSwW];
@@ -423,26 +437,23 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Update of one interior point: off is its offset in the shared planes (the
-// right-hand-side planes start one row later), gi its padded global index
-// (for the map values of faces that cross the surface).  Returns gs - old.
-// Multigrid smoothing divides with the fast reciprocal; the SOR fallback
-// (pb_solver.rs:373-447) with the exact division, as a plain sweep does.
+// Update of one interior point from its six neighbour values, right-hand
+// side and the stencil codes of the point (c0) and of its x-, y- and z-
+// neighbours; gi, gxm: split global indices of the point and of its x - 1
+// neighbour (map values of faces that cross the surface).  Returns the new
+// value; dv = gs - old.  Multigrid smoothing divides with the fast
+// reciprocal; the SOR fallback (pb_solver.rs:373-447) with the exact
+// division, as a plain sweep does.
 template <bool kExact>
-__device__ __forceinline__ float sw_update(const Lv& d, const float4 (*__restrict__ tf)[64], float om,
-                                           float* __restrict__ E0, const float* __restrict__ Em,
-                                           const float* __restrict__ Ep, const float* __restrict__ R,
-                                           const uint8_t* __restrict__ C0, const uint8_t* __restrict__ Cm, int off,
-                                           int gi) {
-  float* ec = E0 + off;
-  const float xm = ec[-1], xp = ec[1], ym = ec[-kSwW], yp = ec[kSwW], zm = Em[off], zp = Ep[off], old = ec[0];
-  const float rhs = R[off - kSwW];
+__device__ __forceinline__ float sw_point(const Lv& d, const float4 (*__restrict__ tf)[64], float om, float old,
+                                          float xp, float xm, float yp, float ym, float zp, float zm, float rhs,
+                                          unsigned c0, unsigned cxm, unsigned cym, unsigned czm, int gi, int gxm,
+                                          float& dv) {
   float ns, dg;
   if (d.uni) {
     ns = d.w6 * ((xp + xm) + (yp + ym) + (zp + zm));
     dg = 6.0f * d.w6;
   } else {
-    const unsigned c0 = C0[off], cxm = C0[off - 1], cym = C0[off - kSwW], czm = Cm[off];
     const float k2 = (c0 & 64u) ? d.kb : 0.0f;
     if (((c0 & 0x2Au) | (cxm & 0x2u) | (cym & 0x8u) | (czm & 0x20u)) == 0u) {  // no face crosses the surface
       const unsigned pat = (c0 & 0x15u) | ((cxm & 0x1u) << 1) | ((cym & 0x4u) << 1) | ((czm & 0x10u) << 1);
@@ -450,7 +461,7 @@ __device__ __forceinline__ float sw_update(const Lv& d, const float4 (*__restric
       ns = ((u.x * xp + u.y * xm) + (u.z * yp + u.w * ym) + (v.x * zp + v.y * zm)) * d.ih;
       dg = fmaf(v.z, d.ih, k2);
     } else {
-      const float a = face(c0 & 3u, d.ex, gi, d.fin, d.fout), b = face(cxm & 3u, d.ex, gi - 1, d.fin, d.fout),
+      const float a = face(c0 & 3u, d.ex, gi, d.fin, d.fout), b = face(cxm & 3u, d.ex, gxm, d.fin, d.fout),
                   c = face((c0 >> 2) & 3u, d.ey, gi, d.fin, d.fout),
                   dd = face((cym >> 2) & 3u, d.ey, gi - d.sy, d.fin, d.fout),
                   f = face((c0 >> 4) & 3u, d.ez, gi, d.fin, d.fout),
@@ -460,9 +471,8 @@ __device__ __forceinline__ float sw_update(const Lv& d, const float4 (*__restric
     }
   }
   const float gs = kExact ? (ns + rhs) / dg : __fdividef(ns + rhs, dg);
-  const float dv = gs - old;
-  ec[0] = old + om * dv;
-  return dv;
+  dv = gs - old;
+  return old + om * dv;
 }
 
 // kSorMode: one sweep of the SOR fallback on the finest level's correction
@@ -470,7 +480,7 @@ __device__ __forceinline__ float sw_update(const Lv& d, const float4 (*__restric
 // block the sum of (gs - old)^2 over the block's own points into
 // part[grid * nparts + block] (halo points are another block's).
 template <bool kSorMode>
-__global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __restrict__ L, int lvl,
+__global__ void __launch_bounds__(kSwThreads, 3) k_sweep_t(WL w, const LvlD* __restrict__ L, int lvl,
                                                         const JobState* __restrict__ S, int flip, int zero_src,
                                                         double* __restrict__ part, int nparts) {
   extern __shared__ __align__(16) unsigned char sw_raw[];  // sizeof(SwSmem), above the 48 KB static limit
@@ -485,108 +495,168 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
   float* __restrict__ dst = flip ? d.e : d.e2;
   const int ntx = (d.nx + kSwTX - 1) / kSwTX, nty = (d.ny + kSwTY - 1) / kSwTY;
   const int bx = lb % ntx, q = lb / ntx, by = q % nty, bz = q / nty;
-  const int xt = bx * kSwTX, yt = by * kSwTY;
+  const int xt = bx * kSwTX, yt = by * kSwTY, hx0 = xt >> 1, hp = d.hp;
   const int z0 = bz * d.zc, z1 = min(z0 + d.zc, d.nz);
   const int tid = threadIdx.x;
 
-  // copy chunks of this thread (shared offset, global offset within a plane; -1: none)
-  auto chunk = [&](int rows, int y0, int& so, int& go) {
+  // copy chunks of this thread: k-th chunk of a plane is (row, half, c);
+  // shared offset and global offset within a plane, -1: none
+  auto chunk = [&](int k, int rows, int y0, int& so, int& go) {
     so = go = -1;
-    if (tid >= rows * (kSwW / 4)) return;
-    const int r = tid / (kSwW / 4), c = tid % (kSwW / 4), y = y0 + r, x = xt - 4 + 4 * c;
-    if (y < 0 || y >= d.ny || x < 0 || x >= d.sy) return;
-    so = r * kSwW + 4 * c;
-    go = x + d.sy * y;
+    if (k >= rows * 2 * kSwChunks) return;
+    const int r = k / (2 * kSwChunks), hh = (k / kSwChunks) & 1, c = k % kSwChunks, y = y0 + r;
+    const int hi = hx0 - 4 + 4 * c;  // first half-index of the chunk
+    if (y < 0 || y >= d.ny || hi < 0 || hi + 4 > hp) return;
+    so = r * kSwW + hh * kSwHW + 4 * c;
+    go = y * d.sy + hh * hp + hi;
   };
-  int eso, ego, rso, rgo, cso, cgo;
-  chunk(kSwEY, yt - 2, eso, ego);
-  chunk(kSwRY, yt - 1, rso, rgo);
-  chunk(kSwCY, yt - 2, cso, cgo);
-  if (d.uni) cso = -1;
-  // ring slot of plane p (p >= -2; two's complement & keeps negatives in range)
+  int eso[2], ego[2], rso[2], rgo[2], cso[2], cgo[2];
+#pragma unroll
+  for (int u = 0; u < 2; u++) {
+    chunk(tid + u * kSwThreads, kSwEY, yt - 2, eso[u], ego[u]);
+    chunk(tid + u * kSwThreads, kSwRY, yt - 1, rso[u], rgo[u]);
+    chunk(tid + u * kSwThreads, kSwCY, yt - 2, cso[u], cgo[u]);
+    if (d.uni) cso[u] = -1;
+  }
   auto se_ = [](int p) { return p & (kSwNE - 1); };
   auto sr_ = [](int p) { return p & (kSwNR - 1); };
   auto sc_ = [](int p) { return p & (kSwNC - 1); };
   auto load_e = [&](int p) {  // zero_src: the correction is zero (first sweep of a cycle on the finest level)
-    if (ego < 0 || p < 0 || p >= d.nz) return;
-    if (zero_src)
-      *(float4*)&sm.e[se_(p)][eso] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    else
-      cp_async16(&sm.e[se_(p)][eso], src + ego + (long long)d.sz * p);
+    if (p < 0 || p >= d.nz) return;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      if (ego[u] < 0) continue;
+      if (zero_src)
+        *(float4*)&sm.e[se_(p)][eso[u]] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      else
+        cp_async16(&sm.e[se_(p)][eso[u]], src + ego[u] + (long long)d.sz * p);
+    }
   };
   auto load_r = [&](int p) {
-    if (rgo >= 0 && p >= 0 && p < d.nz) cp_async16(&sm.r[sr_(p)][rso], d.rhs + rgo + (long long)d.sz * p);
+    if (p < 0 || p >= d.nz) return;
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+      if (rgo[u] >= 0) cp_async16(&sm.r[sr_(p)][rso[u]], d.rhs + rgo[u] + (long long)d.sz * p);
   };
   auto load_c = [&](int p) {
-    if (cso >= 0 && p >= 0 && p < d.nz) cp_async4(&sm.c[sc_(p)][cso], d.cd + cgo + (long long)d.sz * p);
+    if (p < 0 || p >= d.nz) return;
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+      if (cgo[u] >= 0) cp_async4(&sm.c[sc_(p)][cso[u]], d.cd + cgo[u] + (long long)d.sz * p);
   };
-  // this thread's points.  Main (first point): even point of row ym = yt-1+tid/16
-  // at x = xt + 2(tid%16) + ((xt + ym + p) & 1).  Second point: odd point of row
-  // yo = yt + tid/16 at x = xt + 2(tid%16) + ((xt + yo + p + 1) & 1), or for
-  // threads TY*16 .. TY*16+TY+1 the halo even point of row yh = yt-1+(tid-TY*16)
-  // at xt-1 or xt+TX, whichever has the even colour.
-  const int cm = tid & 15;
-  const int ym = yt - 1 + (tid >> 4);
-  const bool m_ok = ym >= 1 && ym <= d.ny - 2;
-  const int m_pb = (xt + ym) & 1, m_off = (ym - yt + 2) * kSwW + 4 + 2 * cm, m_g = xt + 2 * cm + d.sy * ym;
-  int o_kind = 0, o_y = 0, o_pb = 0, o_off = 0, o_g = 0;  // 1 odd point, 2 halo even point
-  if (tid < kSwTY * 16) {
-    o_y = yt + (tid >> 4);
-    o_kind = 1;
-    o_pb = (xt + o_y + 1) & 1;
-    o_off = (o_y - yt + 2) * kSwW + 4 + 2 * cm;
-    o_g = xt + 2 * cm + d.sy * o_y;
-  } else if (tid < kSwTY * 16 + kSwTY + 2) {
-    o_y = yt - 1 + (tid - kSwTY * 16);
-    o_kind = 2;
-    o_pb = (xt - 1 + o_y) & 1;  // 0: x = xt-1 is even-coloured in even planes
-    o_off = (o_y - yt + 2) * kSwW + 3;
-    o_g = xt - 1 + d.sy * o_y;
+  // this thread's update: 0 none, 1 odd quad of plane s, 2 even quad of plane s+2, 3 x-halo even point of s+2
+  int role = 0, uy = 0, uq = 0;
+  if (tid < 64) {
+    role = 1;
+    uy = yt + (tid >> 2);
+    uq = tid & 3;
+  } else if (tid < 136) {
+    role = 2;
+    uy = yt - 1 + ((tid - 64) >> 2);
+    uq = (tid - 64) & 3;
+  } else if (tid < 154) {
+    role = 3;
+    uy = yt - 1 + (tid - 136);
   }
-  if (o_y < 1 || o_y > d.ny - 2) o_kind = 0;
-  // store of this thread: one aligned float4 of a tile row
-  int sso = -1, sgo = 0;
-  if (tid < kSwTY * (kSwTX / 4)) {
-    const int r = tid / (kSwTX / 4), c = tid % (kSwTX / 4), y = yt + r, x = xt + 4 * c;
-    if (y < d.ny && x < d.sy) {
-      sso = (r + 2) * kSwW + 4 * c + 4;
-      sgo = x + d.sy * y;
+  const bool row_ok = uy >= 1 && uy <= d.ny - 2;
+  const bool own_row = uy >= yt && uy < yt + kSwTY;
+  const int er = uy - (yt - 2), rr = uy - (yt - 1), cr = uy - (yt - 2);  // shared rows of this thread's row
+  // the four points of a quad: half h, half-indices hx0 + 4 uq + k
+  auto quad = [&](int p, int h, bool own) {
+    if (p < 1 || p > d.nz - 2 || !row_ok) return;
+    const int hi0 = hx0 + 4 * uq, so = 4 + 4 * uq;  // shared element offset within a half-row
+    float* E0 = sm.e[se_(p)] + er * kSwW;
+    const float* Em = sm.e[se_(p - 1)] + er * kSwW;
+    const float* Ep = sm.e[se_(p + 1)] + er * kSwW;
+    const float* R = sm.r[sr_(p)] + rr * kSwW;
+    const float4 old = *(const float4*)&E0[h * kSwHW + so];
+    const float4 A = *(const float4*)&E0[(1 - h) * kSwHW + so];
+    const float B = E0[(1 - h) * kSwHW + (h ? so + 4 : so - 1)];
+    const float4 yp = *(const float4*)&E0[kSwW + h * kSwHW + so], ym = *(const float4*)&E0[-kSwW + h * kSwHW + so];
+    const float4 zp = *(const float4*)&Ep[h * kSwHW + so], zm = *(const float4*)&Em[h * kSwHW + so];
+    const float4 rh = *(const float4*)&R[h * kSwHW + so];
+    float4 xp, xm;
+    if (h) {  // odd x: x+1 is the next even point, x-1 the even point of the same index
+      xp = make_float4(A.y, A.z, A.w, B);
+      xm = A;
+    } else {  // even x: x+1 is the odd point of the same index, x-1 the previous one
+      xp = A;
+      xm = make_float4(B, A.x, A.y, A.z);
     }
-  }
-  struct Planes {
-    float* E0;
-    const float *Em, *Ep, *R;
-    const uint8_t *C0, *Cm;
-    int gp;
+    unsigned c0 = 0u, cxm = 0u, cym = 0u, czm = 0u;
+    if (!d.uni) {
+      const uint8_t* C0 = sm.c[sc_(p)] + cr * kSwW;
+      const uint8_t* Cm = sm.c[sc_(p - 1)] + cr * kSwW;
+      c0 = *(const unsigned*)&C0[h * kSwHW + so];
+      cym = *(const unsigned*)&C0[-kSwW + h * kSwHW + so];
+      czm = *(const unsigned*)&Cm[h * kSwHW + so];
+      const unsigned w1 = *(const unsigned*)&C0[(1 - h) * kSwHW + so];
+      cxm = h ? w1 : __funnelshift_r(*(const unsigned*)&C0[(1 - h) * kSwHW + so - 4], w1, 24);
+    }
+    const int gb = p * d.sz + uy * d.sy + h * hp + hi0;  // split global index of the first point
+    float o[4] = {old.x, old.y, old.z, old.w};
+    const float vxp[4] = {xp.x, xp.y, xp.z, xp.w}, vxm[4] = {xm.x, xm.y, xm.z, xm.w};
+    const float vyp[4] = {yp.x, yp.y, yp.z, yp.w}, vym[4] = {ym.x, ym.y, ym.z, ym.w};
+    const float vzp[4] = {zp.x, zp.y, zp.z, zp.w}, vzm[4] = {zm.x, zm.y, zm.z, zm.w};
+    const float vr[4] = {rh.x, rh.y, rh.z, rh.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int x = 2 * (hi0 + k) + h;
+      if (x < 1 || x > d.nx - 2) continue;
+      float dv;
+      o[k] = sw_point<kSorMode>(d, sm.tf, om, o[k], vxp[k], vxm[k], vyp[k], vym[k], vzp[k], vzm[k], vr[k],
+                                (c0 >> (8 * k)) & 0xFFu, (cxm >> (8 * k)) & 0xFFu, (cym >> (8 * k)) & 0xFFu,
+                                (czm >> (8 * k)) & 0xFFu, gb + k, ixm(gb + k, x, hp), dv);
+      if (kSorMode && own) acc += (double)dv * (double)dv;
+    }
+    *(float4*)&E0[h * kSwHW + so] = make_float4(o[0], o[1], o[2], o[3]);
   };
-  auto planes = [&](int p) {
-    return Planes{sm.e[se_(p)], sm.e[se_(p - 1)], sm.e[se_(p + 1)], sm.r[sr_(p)],
-                  sm.c[sc_(p)], sm.c[sc_(p - 1)], d.sz * p};
-  };
-  auto update = [&](const Planes& P, int x, int off, int g, bool own) {
+  // the x-halo even point of this thread's row in plane p (never the block's own)
+  auto halo = [&](int p) {
+    if (p < 1 || p > d.nz - 2 || !row_ok) return;
+    const bool right = ((uy + p) & 1) == 0;  // x = xt + 32 (even x) is even-coloured
+    const int x = right ? xt + kSwTX : xt - 1;
     if (x < 1 || x > d.nx - 2) return;
-    const float dv = sw_update<kSorMode>(d, sm.tf, om, P.E0, P.Em, P.Ep, P.R, P.C0, P.Cm, off, g + P.gp);
-    if (kSorMode && own) acc += (double)dv * (double)dv;
-  };
-  const bool m_own = ym >= yt && ym < yt + kSwTY;  // first-point row inside the tile (not the y halo)
-  // even points of plane p: first point and x-halo point
-  auto even = [&](int p) {
-    if (p < 1 || p > d.nz - 2) return;
-    const Planes P = planes(p);
-    const int par = m_pb ^ (p & 1);
-    const bool own = p >= z0 && p < z1;
-    if (m_ok) update(P, xt + 2 * cm + par, m_off + par, m_g + par, own && m_own);
-    if (o_kind == 2) {
-      const int h = (o_pb ^ (p & 1)) ? kSwTX + 1 : 0;  // xt-1 or xt+TX
-      update(P, xt - 1 + h, o_off + h, o_g + h, false);
+    const int h = x & 1, so = (x >> 1) - hx0 + 4;  // 20 (even half) or 3 (odd half)
+    float* E0 = sm.e[se_(p)] + er * kSwW;
+    const float* Em = sm.e[se_(p - 1)] + er * kSwW;
+    const float* Ep = sm.e[se_(p + 1)] + er * kSwW;
+    const float* R = sm.r[sr_(p)] + rr * kSwW;
+    // x+1 / x-1 in the other half: even x -> odd indices so, so-1; odd x -> even indices so+1, so
+    const int op = (1 - h) * kSwHW + (h ? so + 1 : so), om_ = (1 - h) * kSwHW + (h ? so : so - 1);
+    const int me = h * kSwHW + so;
+    unsigned c0 = 0u, cxm = 0u, cym = 0u, czm = 0u;
+    if (!d.uni) {
+      const uint8_t* C0 = sm.c[sc_(p)] + cr * kSwW;
+      const uint8_t* Cm = sm.c[sc_(p - 1)] + cr * kSwW;
+      c0 = C0[me];
+      cxm = C0[om_];
+      cym = C0[me - kSwW];
+      czm = Cm[me];
     }
+    const int gi = p * d.sz + uy * d.sy + xo(x, hp);
+    float dv;
+    E0[me] = sw_point<kSorMode>(d, sm.tf, om, E0[me], E0[op], E0[om_], E0[me + kSwW], E0[me - kSwW], Ep[me], Em[me],
+                                R[me], c0, cxm, cym, czm, gi, ixm(gi, x, hp), dv);
+  };
+  auto even = [&](int p) {
+    if (role == 2)
+      quad(p, (uy + p) & 1, own_row && p >= z0 && p < z1);
+    else if (role == 3)
+      halo(p);
   };
   auto odd = [&](int p) {
-    if (o_kind != 1 || p < 1 || p > d.nz - 2) return;
-    const Planes P = planes(p);
-    const int par = o_pb ^ (p & 1);
-    update(P, xt + 2 * cm + par, o_off + par, o_g + par, true);
+    if (role == 1) quad(p, (1 + uy + p) & 1, own_row);
   };
+  // store of this thread: one float4 of a tile row half
+  int sso = -1, sgo = 0;
+  if (tid < kSwTY * 2 * 4) {
+    const int r = tid >> 3, hh = (tid >> 2) & 1, c = tid & 3, y = yt + r, hi = hx0 + 4 * c;
+    if (y < d.ny && hi + 4 <= hp) {
+      sso = (r + 2) * kSwW + hh * kSwHW + 4 + 4 * c;
+      sgo = y * d.sy + hh * hp + hi;
+    }
+  }
   auto store = [&](int p) {
     if (sso >= 0) *(float4*)(dst + sgo + (long long)d.sz * p) = *(const float4*)&sm.e[se_(p)][sso];
   };
@@ -633,7 +703,6 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
     if (threadIdx.x == 0) part[(long long)j * nparts + lb] = t;
   }
 }
-
 
 // SOR bookkeeping after a sweep and its update (pb_solver.rs:373-447): rms
 // of the sweep's updates from the sweep blocks' partial sums (fixed order),
@@ -683,9 +752,9 @@ __global__ void __launch_bounds__(256) k_res32(WL w, const LvlD* __restrict__ L,
   for (int k = 0; k < 8; k++) {
     int z = z0 + k;
     if (z < 1 || z > d.nz - 2) continue;
-    int i = x + d.sy * y + d.sz * z;
+    int i = xo(x, d.hp) + d.sy * y + d.sz * z;
     float ns, dg;
-    st32(d, d.e2, i, ns, dg);
+    st32(d, d.e2, x, i, ns, dg);
     d.res[i] = d.rhs[i] + ns - dg * d.e2[i];
   }
 }
@@ -722,12 +791,12 @@ __global__ void __launch_bounds__(256) k_restrict32(WL w, const LvlD* __restrict
           int x = fx + dx;
           if (x < 0 || x >= f.nx) continue;
           float wt = wyz * (dx == 0 ? 2.0f : 1.0f);
-          sum += wt * res[x + f.sy * y + f.sz * z];
+          sum += wt * res[xo(x, f.hp) + f.sy * y + f.sz * z];
           ws += wt;
         }
       }
     }
-    int i = cx + c.sy * cy + c.sz * cz;
+    int i = xo(cx, c.hp) + c.sy * cy + c.sz * cz;
     c.rhs[i] = rsc * sum / ws;
     c.e[i] = 0.0f;
   }
@@ -757,13 +826,14 @@ __global__ void __launch_bounds__(256) k_prolong32(WL w, const LvlD* __restrict_
     if (fz >= f.nz || (skipb && (fz == 0 || fz == f.nz - 1))) continue;
     int z0 = min(fz >> 1, mz);
     float dz = (float)fz * 0.5f - (float)z0;
-    const float* b = ce + x0 + c.sy * y0 + c.sz * z0;
-    float c00 = b[0] * (1.0f - dx) + b[1] * dx;
-    float c10 = b[c.sy] * (1.0f - dx) + b[c.sy + 1] * dx;
-    float c01 = b[c.sz] * (1.0f - dx) + b[c.sz + 1] * dx;
-    float c11 = b[c.sz + c.sy] * (1.0f - dx) + b[c.sz + c.sy + 1] * dx;
+    const float* b = ce + c.sy * y0 + c.sz * z0;
+    const int a0 = xo(x0, c.hp), a1 = xo(x0 + 1, c.hp);
+    float c00 = b[a0] * (1.0f - dx) + b[a1] * dx;
+    float c10 = b[c.sy + a0] * (1.0f - dx) + b[c.sy + a1] * dx;
+    float c01 = b[c.sz + a0] * (1.0f - dx) + b[c.sz + a1] * dx;
+    float c11 = b[c.sz + c.sy + a0] * (1.0f - dx) + b[c.sz + c.sy + a1] * dx;
     float c0 = c00 * (1.0f - dy) + c10 * dy, c1 = c01 * (1.0f - dy) + c11 * dy;
-    f.e2[fx + f.sy * fy + f.sz * fz] += c0 * (1.0f - dz) + c1 * dz;
+    f.e2[xo(fx, f.hp) + f.sy * fy + f.sz * fz] += c0 * (1.0f - dz) + c1 * dz;
   }
 }
 
@@ -780,9 +850,9 @@ __global__ void k_coarse32(WL w, const LvlD* __restrict__ L, int lvl, const JobS
       for (int k = threadIdx.x; k < ni; k += blockDim.x) {
         int ix = 1 + k % nxi, iy = 1 + (k / nxi) % nyi, iz = 1 + k / (nxi * nyi);
         if (((ix + iy + iz + colour) & 1) != 0) continue;
-        int i = ix + d.sy * iy + d.sz * iz;
+        int i = xo(ix, d.hp) + d.sy * iy + d.sz * iz;
         float ns, dg;
-        st32(d, d.e, i, ns, dg);
+        st32(d, d.e, ix, i, ns, dg);
         float old = d.e[i];
         float gs = (ns + d.rhs[i]) / dg;
         d.e[i] = old + d.om * (gs - old);
@@ -895,7 +965,7 @@ __global__ void k_maps32(WL w, const JobD* __restrict__ J, const LvlD* __restric
   int n = d.nx * d.ny * d.nz;
   int i = lb * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const long long ci = i % d.nx + (long long)d.px * (i / d.nx);  // padded FP32 index
+  const long long ci = xo(i % d.nx, d.px >> 1) + (long long)d.px * (i / d.nx);  // split FP32 index
   ((float*)l0.ex)[ci] = (float)d.ex[i];
   ((float*)l0.ey)[ci] = (float)d.ey[i];
   ((float*)l0.ez)[ci] = (float)d.ez[i];
@@ -918,7 +988,7 @@ __global__ void k_codes(WL w, const JobD* __restrict__ J, const LvlD* __restrict
   unsigned exc = 0, chg = 0;
   if (i < n) {
     const int x = i % d.nx, t = i / d.nx;
-    const long long ci = x + (long long)d.px * t;  // t = y + ny z
+    const long long ci = xo(x, d.px >> 1) + (long long)d.px * t;  // t = y + ny z
     unsigned c = 0;
     if (!d.uniform) {
       unsigned a = fcode(d.ex[i], d.din, d.dout), b = fcode(d.ey[i], d.din, d.dout), e = fcode(d.ez[i], d.din, d.dout);
@@ -954,8 +1024,8 @@ __global__ void k_inject32(WL w, const LvlD* __restrict__ L, int lvl) {
   int i = lb * blockDim.x + threadIdx.x;
   if (i >= cn) return;
   int cx = i % c.nx, cy = (i / c.nx) % c.ny, cz = i / (c.nx * c.ny);
-  int fi = min(2 * cx, f.nx - 1) + f.px * (min(2 * cy, f.ny - 1) + f.ny * min(2 * cz, f.nz - 1));
-  int ci = cx + c.px * (cy + c.ny * cz);
+  int fi = xo(min(2 * cx, f.nx - 1), f.px >> 1) + f.px * (min(2 * cy, f.ny - 1) + f.ny * min(2 * cz, f.nz - 1));
+  int ci = xo(cx, c.px >> 1) + c.px * (cy + c.ny * cz);
   ((float*)c.ex)[ci] = f.ex[fi];
   ((float*)c.ey)[ci] = f.ey[fi];
   ((float*)c.ez)[ci] = f.ez[fi];
@@ -983,7 +1053,8 @@ __device__ __forceinline__ float coarse_face(const LvlD& f, const float* __restr
       if (p[t1] < 0 || p[t1] >= n[t1] || p[t2] < 0 || p[t2] >= n[t2]) continue;
       int q[3] = {p[0], p[1], p[2]};
       q[axis] = min(p[axis] + 1, n[axis] - 1);
-      const float e0 = m[p[0] + f.px * (p[1] + f.ny * p[2])], e1 = m[q[0] + f.px * (q[1] + f.ny * q[2])];
+      const float e0 = m[xo(p[0], f.px >> 1) + f.px * (p[1] + f.ny * p[2])],
+                  e1 = m[xo(q[0], f.px >> 1) + f.px * (q[1] + f.ny * q[2])];
       if (!any) first = e0;
       any = true;
       same = same && e0 == first && e1 == first;
@@ -1005,8 +1076,8 @@ __global__ void k_coarsen32(WL w, const LvlD* __restrict__ L, int lvl) {
   if (i >= cn) return;
   int cx = i % c.nx, cy = (i / c.nx) % c.ny, cz = i / (c.nx * c.ny);
   int bx = min(2 * cx, f.nx - 1), by = min(2 * cy, f.ny - 1), bz = min(2 * cz, f.nz - 1);
-  int fi = bx + f.px * (by + f.ny * bz);
-  int ci = cx + c.px * (cy + c.ny * cz);
+  int fi = xo(bx, f.px >> 1) + f.px * (by + f.ny * bz);
+  int ci = xo(cx, c.px >> 1) + c.px * (cy + c.ny * cz);
   const float ex = coarse_face(f, f.ex, 0, bx, by, bz), ey = coarse_face(f, f.ey, 1, bx, by, bz),
               ez = coarse_face(f, f.ez, 2, bx, by, bz);
   ((float*)c.ex)[ci] = ex;
@@ -1079,7 +1150,8 @@ F64Lay f64_lay(const PbJob& J) {
   return f;
 }
 // FP32 and code arrays: rows padded to a multiple of 4 points (16 bytes of FP32)
-int pitch(const PbGeom& g) { return (int)((g.nx + 3) & ~3); }
+// split rows (see xo): half pitch = the even points of a row rounded up to 4
+int pitch(const PbGeom& g) { return 2 * (int)((((g.nx + 1) >> 1) + 3) & ~3); }
 size_t padded_n(const PbGeom& g) { return (size_t)pitch(g) * g.ny * g.nz; }
 
 long long nbricks(const PbGeom& g) { return cdiv(g.nx, 32) * cdiv(g.ny, 8) * cdiv(g.nz, 8); }
@@ -1217,6 +1289,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   double* P64 = pool64_.as<double>();
   float* P32 = pool32_.as<float>();
   RSTG_CUDA(cudaMemsetAsync(P32, 0, b32, st));
+  RSTG_CUDA(cudaMemsetAsync(P8, 0, b8, st));  // split rows: padding codes are read (and ignored) with their row
 
   // ---- maps and boundary values (FP64, the reference's set-up) -------------
   // One grid's set-up is a chain of small launches with host waits (the
