@@ -380,8 +380,9 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
 // the updated even ones, each point with the arithmetic of the
 // single-colour update.  A block owns an x-y tile of 32 x 16 points and
 // marches a chunk of z planes.  Planes of the correction (with a two-row
-// halo), of the right-hand side and of the stencil codes stream into
-// shared-memory rings with cp.async, two steps ahead of their use.  Step s
+// halo) and of the stencil codes stream into shared-memory rings with
+// cp.async, two steps ahead of their use; the right-hand side, which one
+// thread reads per point, streams through registers one step ahead.  Step s
 // updates, in one phase between barriers, the even points of plane s+2 over
 // the tile and a one-point halo, the odd points of plane s (whose even
 // neighbours in planes s-1 .. s+1 are already updated) and writes plane s-1
@@ -394,30 +395,42 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
 // them with 16-byte loads of the point values, of each of the y / z
 // neighbour rows, of the right-hand side and of the other half (the x
 // neighbours), and 4-byte loads of four stencil codes.  160 threads: 64
-// update four odd points of plane s each (16 rows x 4 quads), 72 four even
-// points of plane s+2 (18 rows: the tile and a y halo row on each side), 18
-// the even point of the x halo of a row (x = xt-1 or xt+32, whichever is
-// even-coloured).
+// update four odd points of plane s each (16 rows x 4 quads), 90 four even
+// points of plane s+2 (18 rows: the tile and a y halo row on each side; five
+// quads a row, the fifth for the row's x-halo point, x = xt-1 or xt+32,
+// whichever is even-coloured).  The quads 0..3 of a quarter warp lie in rows
+// r and r + 2, whose points have the same colour parity; with shared rows of
+// 56 floats those rows start 16 banks apart, so each 16-byte load of a
+// quarter warp touches every bank once.
+constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 160, kSwZC0 = 24, kSwZC1 = 16;
 // z planes per block: long marches on the finest level, short ones on the
-// coarse levels (few tiles per grid there, so more chunks keep the SMs busy)
-constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 160, kSwZC0 = 48, kSwZC1 = 16;
-int sweep_chunk(int lvl) { return lvl == 0 ? kSwZC0 : (lvl == 1 ? kSwZC1 : 8); }
+// coarse levels (few tiles per grid there, so more chunks keep the SMs busy);
+// a grid's planes are dealt evenly over its chunks
+__host__ __device__ inline int sweep_zc(int lvl, int nz) {
+  const int base = lvl == 0 ? kSwZC0 : (lvl == 1 ? kSwZC1 : 8);
+  const int k = nz > base ? (nz + base - 1) / base : 1;
+  return nz > 0 ? (nz + k - 1) / k : 1;
+}
+__host__ __device__ inline int sweep_blocks(int lvl, int nx, int ny, int nz) {
+  const int zc = sweep_zc(lvl, nz);
+  return ((nx + kSwTX - 1) / kSwTX) * ((ny + kSwTY - 1) / kSwTY) * ((nz + zc - 1) / zc);
+}
 constexpr int kSwHW = 24;         // shared half-row: half-indices [hx0-4, hx0+20), hx0 = xt/2
-constexpr int kSwW = 2 * kSwHW;   // shared row: even half, then odd half
+constexpr int kSwW = 56;          // shared correction row: even half, odd half, 8 floats of padding
+constexpr int kSwCW = 2 * kSwHW;  // shared code row (bytes): even half, odd half
 constexpr int kSwEY = kSwTY + 4;  // correction rows: y in [yt-2, yt+TY+2)
-constexpr int kSwRY = kSwTY + 2;  // right-hand-side rows: y in [yt-1, yt+TY+1)
 constexpr int kSwCY = kSwTY + 3;  // code rows: y in [yt-2, yt+TY+1)
-constexpr int kSwNE = 8, kSwNR = 8, kSwNC = 8;  // ring depths in planes (slot = plane & (depth - 1))
-constexpr int kSwChunks = kSwHW / 4;           // 16-byte (or 4-code) chunks per half-row
+constexpr int kSwNE = 8, kSwNC = 8;   // ring depths in planes (slot = plane & (depth - 1))
+constexpr int kSwChunks = kSwHW / 4;  // 16-byte (or 4-code) chunks per half-row
 static_assert(kSwTX == 32 && kSwTY == 16, "thread roles of the sweep");
-static_assert(kSwEY * 2 * kSwChunks <= 2 * kSwThreads && kSwRY * 2 * kSwChunks <= 2 * kSwThreads &&
-                  kSwCY * 2 * kSwChunks <= 2 * kSwThreads && kSwTY * 2 * 4 <= kSwThreads,
+static_assert((2 * kSwW) % 32 == 16 && kSwW >= 2 * kSwHW, "rows r and r + 2 start 16 banks apart");
+static_assert(kSwEY * 2 * kSwChunks <= 2 * kSwThreads && kSwCY * 2 * kSwChunks <= 2 * kSwThreads &&
+                  kSwTY * 2 * 4 <= kSwThreads,
               "two copy chunks and one store per thread and plane");
 
 struct SwSmem {
   float e[kSwNE][kSwEY * kSwW];
-  float r[kSwNR][kSwRY * kSwW];
-  uint8_t c[kSwNC][kSwCY * kSwW];
+  uint8_t c[kSwNC][kSwCY * kSwCW];
   // faces of every eps_in / eps_out pattern (bit k set: face k is eps_in;
   // faces x+, x-, y+, y-, z+, z-): [0] x+, x-, y+, y-; [1] z+, z-, their sum
   float4 tf[2][64];
@@ -437,53 +450,25 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Update of one interior point from its six neighbour values, right-hand
-// side and the stencil codes of the point (c0) and of its x-, y- and z-
-// neighbours; gi, gxm: split global indices of the point and of its x - 1
-// neighbour (map values of faces that cross the surface).  Returns the new
-// value; dv = gs - old.  Multigrid smoothing divides with the fast
-// reciprocal; the SOR fallback (pb_solver.rs:373-447) with the exact
-// division, as a plain sweep does.
-template <bool kExact>
-__device__ __forceinline__ float sw_point(const Lv& d, const float4 (*__restrict__ tf)[64], float om, float old,
-                                          float xp, float xm, float yp, float ym, float zp, float zm, float rhs,
-                                          unsigned c0, unsigned cxm, unsigned cym, unsigned czm, int gi, int gxm,
-                                          float& dv) {
-  float ns, dg;
-  if (d.uni) {
-    ns = d.w6 * ((xp + xm) + (yp + ym) + (zp + zm));
-    dg = 6.0f * d.w6;
-  } else {
-    const float k2 = (c0 & 64u) ? d.kb : 0.0f;
-    if (((c0 & 0x2Au) | (cxm & 0x2u) | (cym & 0x8u) | (czm & 0x20u)) == 0u) {  // no face crosses the surface
-      const unsigned pat = (c0 & 0x15u) | ((cxm & 0x1u) << 1) | ((cym & 0x4u) << 1) | ((czm & 0x10u) << 1);
-      const float4 u = tf[0][pat], v = tf[1][pat];
-      ns = ((u.x * xp + u.y * xm) + (u.z * yp + u.w * ym) + (v.x * zp + v.y * zm)) * d.ih;
-      dg = fmaf(v.z, d.ih, k2);
-    } else {
-      const float a = face(c0 & 3u, d.ex, gi, d.fin, d.fout), b = face(cxm & 3u, d.ex, gxm, d.fin, d.fout),
-                  c = face((c0 >> 2) & 3u, d.ey, gi, d.fin, d.fout),
-                  dd = face((cym >> 2) & 3u, d.ey, gi - d.sy, d.fin, d.fout),
-                  f = face((c0 >> 4) & 3u, d.ez, gi, d.fin, d.fout),
-                  g = face((czm >> 4) & 3u, d.ez, gi - d.sz, d.fin, d.fout);
-      ns = ((a * xp + b * xm) + (c * yp + dd * ym) + (f * zp + g * zm)) * d.ih;
-      dg = fmaf((a + b) + (c + dd) + (f + g), d.ih, k2);
-    }
-  }
-  const float gs = kExact ? (ns + rhs) / dg : __fdividef(ns + rhs, dg);
-  dv = gs - old;
-  return old + om * dv;
-}
+// The update of one interior point (pb_solver.rs:250-317), in quad() below:
+// ns = sum over the six faces of eps_face * neighbour / h^2, dg = sum of
+// eps_face / h^2 (+ kappa-bar^2 where the point's kappa flag is set),
+// gs = (ns + rhs) / dg, new = old + omega (gs - old).  A face dielectric is
+// eps_out, eps_in or, where the face crosses the surface, the map value; the
+// first two come from tf by the point's six eps_in bits and the map faces
+// replace them.  Multigrid smoothing divides with the fast reciprocal; the
+// SOR fallback (pb_solver.rs:373-447) with the exact division, as a plain
+// sweep does.
 
 // kSorMode: one sweep of the SOR fallback on the finest level's correction
 // equation from e = 0 (zero_src), with the grid's Chebyshev omega, and per
 // block the sum of (gs - old)^2 over the block's own points into
 // part[grid * nparts + block] (halo points are another block's).
 template <bool kSorMode>
-__global__ void __launch_bounds__(kSwThreads, 3) k_sweep_t(WL w, const LvlD* __restrict__ L, int lvl,
+__global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __restrict__ L, int lvl,
                                                         const JobState* __restrict__ S, int flip, int zero_src,
                                                         double* __restrict__ part, int nparts) {
-  extern __shared__ __align__(16) unsigned char sw_raw[];  // sizeof(SwSmem), above the 48 KB static limit
+  extern __shared__ __align__(16) unsigned char sw_raw[];  // sizeof(SwSmem)
   SwSmem& sm = *reinterpret_cast<SwSmem*>(sw_raw);
   __shared__ double red[32];
   int lb, j = wl_job(w, blockIdx.x, lb);
@@ -500,26 +485,24 @@ __global__ void __launch_bounds__(kSwThreads, 3) k_sweep_t(WL w, const LvlD* __r
   const int tid = threadIdx.x;
 
   // copy chunks of this thread: k-th chunk of a plane is (row, half, c);
-  // shared offset and global offset within a plane, -1: none
-  auto chunk = [&](int k, int rows, int y0, int& so, int& go) {
+  // shared offset (row stride `stride`) and global offset within a plane, -1: none
+  auto chunk = [&](int k, int rows, int y0, int stride, int& so, int& go) {
     so = go = -1;
     if (k >= rows * 2 * kSwChunks) return;
     const int r = k / (2 * kSwChunks), hh = (k / kSwChunks) & 1, c = k % kSwChunks, y = y0 + r;
     const int hi = hx0 - 4 + 4 * c;  // first half-index of the chunk
     if (y < 0 || y >= d.ny || hi < 0 || hi + 4 > hp) return;
-    so = r * kSwW + hh * kSwHW + 4 * c;
+    so = r * stride + hh * kSwHW + 4 * c;
     go = y * d.sy + hh * hp + hi;
   };
-  int eso[2], ego[2], rso[2], rgo[2], cso[2], cgo[2];
+  int eso[2], ego[2], cso[2], cgo[2];
 #pragma unroll
   for (int u = 0; u < 2; u++) {
-    chunk(tid + u * kSwThreads, kSwEY, yt - 2, eso[u], ego[u]);
-    chunk(tid + u * kSwThreads, kSwRY, yt - 1, rso[u], rgo[u]);
-    chunk(tid + u * kSwThreads, kSwCY, yt - 2, cso[u], cgo[u]);
-    if (d.uni) cso[u] = -1;
+    chunk(tid + u * kSwThreads, kSwEY, yt - 2, kSwW, eso[u], ego[u]);
+    chunk(tid + u * kSwThreads, kSwCY, yt - 2, kSwCW, cso[u], cgo[u]);
+    if (d.uni) cso[u] = cgo[u] = -1;  // constant-coefficient grids read no codes (coarse levels have none)
   }
   auto se_ = [](int p) { return p & (kSwNE - 1); };
-  auto sr_ = [](int p) { return p & (kSwNR - 1); };
   auto sc_ = [](int p) { return p & (kSwNC - 1); };
   auto load_e = [&](int p) {  // zero_src: the correction is zero (first sweep of a cycle on the finest level)
     if (p < 0 || p >= d.nz) return;
@@ -532,49 +515,60 @@ __global__ void __launch_bounds__(kSwThreads, 3) k_sweep_t(WL w, const LvlD* __r
         cp_async16(&sm.e[se_(p)][eso[u]], src + ego[u] + (long long)d.sz * p);
     }
   };
-  auto load_r = [&](int p) {
-    if (p < 0 || p >= d.nz) return;
-#pragma unroll
-    for (int u = 0; u < 2; u++)
-      if (rgo[u] >= 0) cp_async16(&sm.r[sr_(p)][rso[u]], d.rhs + rgo[u] + (long long)d.sz * p);
-  };
   auto load_c = [&](int p) {
     if (p < 0 || p >= d.nz) return;
 #pragma unroll
     for (int u = 0; u < 2; u++)
-      if (cgo[u] >= 0) cp_async4(&sm.c[sc_(p)][cso[u]], d.cd + cgo[u] + (long long)d.sz * p);
+      if (cso[u] >= 0 && cgo[u] >= 0) cp_async4(&sm.c[sc_(p)][cso[u]], d.cd + cgo[u] + (long long)d.sz * p);
   };
-  // this thread's update: 0 none, 1 odd quad of plane s, 2 even quad of plane s+2, 3 x-halo even point of s+2
-  int role = 0, uy = 0, uq = 0;
+  // this thread's update: 0 none, 1 odd quad of plane s, 2 even quad of plane
+  // s+2.  Quads 0..3 of a row cover the tile's 16 points of one colour; an
+  // even row's quad 4 covers its x-halo point (x = xt+32 in the even half or
+  // x = xt-1 in the odd half, whichever is even-coloured) and three more
+  // points that are computed but neither stored nor read.  A thread of quads
+  // 0..3 takes quad (lane & 3) of row 2 ((lane >> 2) & 3) + (lane >> 4) among
+  // its warp's eight rows.
+  const int lane = tid & 31, lrow = 2 * ((lane >> 2) & 3) + (lane >> 4);
+  int role = 0, uy = 0, uq = lane & 3;
   if (tid < 64) {
     role = 1;
-    uy = yt + (tid >> 2);
-    uq = tid & 3;
+    uy = yt + 8 * (tid >> 5) + lrow;
+  } else if (tid < 128) {
+    role = 2;
+    uy = yt - 1 + 8 * ((tid - 64) >> 5) + lrow;
   } else if (tid < 136) {
     role = 2;
-    uy = yt - 1 + ((tid - 64) >> 2);
-    uq = (tid - 64) & 3;
+    uy = yt + 15 + ((tid - 128) >> 2);
   } else if (tid < 154) {
-    role = 3;
+    role = 2;
     uy = yt - 1 + (tid - 136);
+    uq = 4;
   }
-  const bool row_ok = uy >= 1 && uy <= d.ny - 2;
-  const bool own_row = uy >= yt && uy < yt + kSwTY;
-  const int er = uy - (yt - 2), rr = uy - (yt - 1), cr = uy - (yt - 2);  // shared rows of this thread's row
-  // the four points of a quad: half h, half-indices hx0 + 4 uq + k
-  auto quad = [&](int p, int h, bool own) {
-    if (p < 1 || p > d.nz - 2 || !row_ok) return;
-    const int hi0 = hx0 + 4 * uq, so = 4 + 4 * uq;  // shared element offset within a half-row
+  const bool row_act = role != 0 && uy >= 1 && uy <= d.ny - 2;  // interior row
+  const bool own_row = uq < 4 && uy >= yt && uy < yt + kSwTY;
+  const int er = uy - (yt - 2);  // shared correction and code row of this thread's row
+  // shared element offset within a half-row of this thread's quad in half h
+  // (its first half-index is hx0 - 4 + offset)
+  auto qso = [&](int h) { return uq < 4 ? 4 + 4 * uq : (h ? 0 : 20); };
+  // the right-hand side of this thread's update of plane p (zero where it has none)
+  auto rhs_at = [&](int p) {
+    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const int h = role == 1 ? (1 + uy + p) & 1 : (uy + p) & 1, hi0 = hx0 - 4 + qso(h);
+    if (!row_act || p < 1 || p > d.nz - 2 || hi0 < 0 || hi0 >= hp) return v;
+    return __ldg(reinterpret_cast<const float4*>(d.rhs + (long long)d.sz * p + uy * d.sy + h * hp + hi0));
+  };
+  // the four points of a quad: half h, half-indices hi0 + k
+  auto quad = [&](int p, int h, bool own, const float4& rh) {
+    const int so = qso(h), hi0 = hx0 - 4 + so;
+    if (!row_act || p < 1 || p > d.nz - 2 || hi0 < 0 || hi0 >= hp) return;
     float* E0 = sm.e[se_(p)] + er * kSwW;
     const float* Em = sm.e[se_(p - 1)] + er * kSwW;
     const float* Ep = sm.e[se_(p + 1)] + er * kSwW;
-    const float* R = sm.r[sr_(p)] + rr * kSwW;
     const float4 old = *(const float4*)&E0[h * kSwHW + so];
     const float4 A = *(const float4*)&E0[(1 - h) * kSwHW + so];
     const float B = E0[(1 - h) * kSwHW + (h ? so + 4 : so - 1)];
     const float4 yp = *(const float4*)&E0[kSwW + h * kSwHW + so], ym = *(const float4*)&E0[-kSwW + h * kSwHW + so];
     const float4 zp = *(const float4*)&Ep[h * kSwHW + so], zm = *(const float4*)&Em[h * kSwHW + so];
-    const float4 rh = *(const float4*)&R[h * kSwHW + so];
     float4 xp, xm;
     if (h) {  // odd x: x+1 is the next even point, x-1 the even point of the same index
       xp = make_float4(A.y, A.z, A.w, B);
@@ -583,75 +577,79 @@ __global__ void __launch_bounds__(kSwThreads, 3) k_sweep_t(WL w, const LvlD* __r
       xp = A;
       xm = make_float4(B, A.x, A.y, A.z);
     }
-    unsigned c0 = 0u, cxm = 0u, cym = 0u, czm = 0u;
-    if (!d.uni) {
-      const uint8_t* C0 = sm.c[sc_(p)] + cr * kSwW;
-      const uint8_t* Cm = sm.c[sc_(p - 1)] + cr * kSwW;
-      c0 = *(const unsigned*)&C0[h * kSwHW + so];
-      cym = *(const unsigned*)&C0[-kSwW + h * kSwHW + so];
-      czm = *(const unsigned*)&Cm[h * kSwHW + so];
-      const unsigned w1 = *(const unsigned*)&C0[(1 - h) * kSwHW + so];
-      cxm = h ? w1 : __funnelshift_r(*(const unsigned*)&C0[(1 - h) * kSwHW + so - 4], w1, 24);
-    }
     const int gb = p * d.sz + uy * d.sy + h * hp + hi0;  // split global index of the first point
     float o[4] = {old.x, old.y, old.z, old.w};
     const float vxp[4] = {xp.x, xp.y, xp.z, xp.w}, vxm[4] = {xm.x, xm.y, xm.z, xm.w};
     const float vyp[4] = {yp.x, yp.y, yp.z, yp.w}, vym[4] = {ym.x, ym.y, ym.z, ym.w};
     const float vzp[4] = {zp.x, zp.y, zp.z, zp.w}, vzm[4] = {zm.x, zm.y, zm.z, zm.w};
     const float vr[4] = {rh.x, rh.y, rh.z, rh.w};
+    // point k (x = lo + 2k) is interior when k <= kmax and x >= 1
+    const int lo = 2 * hi0 + h, kmax = (d.nx - 2 - lo) >> 1;
+    const bool k0 = lo >= 1;
+    if (d.uni) {
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const int x = 2 * (hi0 + k) + h;
-      if (x < 1 || x > d.nx - 2) continue;
-      float dv;
-      o[k] = sw_point<kSorMode>(d, sm.tf, om, o[k], vxp[k], vxm[k], vyp[k], vym[k], vzp[k], vzm[k], vr[k],
-                                (c0 >> (8 * k)) & 0xFFu, (cxm >> (8 * k)) & 0xFFu, (cym >> (8 * k)) & 0xFFu,
-                                (czm >> (8 * k)) & 0xFFu, gb + k, ixm(gb + k, x, hp), dv);
-      if (kSorMode && own) acc += (double)dv * (double)dv;
+      for (int k = 0; k < 4; k++) {
+        if (k > kmax || (k == 0 && !k0)) continue;
+        const float ns = d.w6 * ((vxp[k] + vxm[k]) + (vyp[k] + vym[k]) + (vzp[k] + vzm[k]));
+        const float dg = 6.0f * d.w6;
+        const float gs = kSorMode ? (ns + vr[k]) / dg : __fdividef(ns + vr[k], dg);
+        const float dv = gs - o[k];
+        o[k] = o[k] + om * dv;
+        if (kSorMode && own) acc += (double)dv * (double)dv;
+      }
+    } else {
+      const uint8_t* C0 = sm.c[sc_(p)] + er * kSwCW;
+      const uint8_t* Cm = sm.c[sc_(p - 1)] + er * kSwCW;
+      const unsigned c0 = *(const unsigned*)&C0[h * kSwHW + so];
+      const unsigned cym = *(const unsigned*)&C0[-kSwCW + h * kSwHW + so];
+      const unsigned czm = *(const unsigned*)&Cm[h * kSwHW + so];
+      const unsigned w1 = *(const unsigned*)&C0[(1 - h) * kSwHW + so];
+      const unsigned cxm = h ? w1 : __funnelshift_r(*(const unsigned*)&C0[(1 - h) * kSwHW + so - 4], w1, 24);
+      // per point (one byte each): the eps_in bits of its six faces, an index
+      // into tf, and whether a face crosses the surface (2-bit face code 2:
+      // the dielectric comes from the maps)
+      const unsigned pat =
+          (c0 & 0x15151515u) | (((cxm & 0x01010101u) | (cym & 0x04040404u) | (czm & 0x10101010u)) << 1);
+      const unsigned crs = (c0 & 0x2A2A2A2Au) | (cxm & 0x02020202u) | (cym & 0x08080808u) | (czm & 0x20202020u);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (k > kmax || (k == 0 && !k0)) continue;
+        const unsigned pk = (pat >> (8 * k)) & 63u;
+        const float4 u = sm.tf[0][pk], v = sm.tf[1][pk];
+        float a = u.x, b = u.y, c = u.z, dd = u.w, f = v.x, g = v.y, sum = v.z;
+        if ((crs >> (8 * k)) & 0xFFu) {
+          const int gi = gb + k;
+          const unsigned q0 = c0 >> (8 * k), qx = cxm >> (8 * k), qy = cym >> (8 * k), qz = czm >> (8 * k);
+          if (q0 & 2u) a = d.ex[gi];
+          if (qx & 2u) b = d.ex[ixm(gi, lo + 2 * k, hp)];
+          if (q0 & 8u) c = d.ey[gi];
+          if (qy & 8u) dd = d.ey[gi - d.sy];
+          if (q0 & 32u) f = d.ez[gi];
+          if (qz & 32u) g = d.ez[gi - d.sz];
+          sum = (a + b) + (c + dd) + (f + g);
+        }
+        const float ns = ((a * vxp[k] + b * vxm[k]) + (c * vyp[k] + dd * vym[k]) + (f * vzp[k] + g * vzm[k])) * d.ih;
+        const float dg = fmaf(sum, d.ih, ((c0 >> (8 * k)) & 64u) ? d.kb : 0.0f);
+        const float gs = kSorMode ? (ns + vr[k]) / dg : __fdividef(ns + vr[k], dg);
+        const float dv = gs - o[k];
+        o[k] = o[k] + om * dv;
+        if (kSorMode && own) acc += (double)dv * (double)dv;
+      }
     }
     *(float4*)&E0[h * kSwHW + so] = make_float4(o[0], o[1], o[2], o[3]);
   };
-  // the x-halo even point of this thread's row in plane p (never the block's own)
-  auto halo = [&](int p) {
-    if (p < 1 || p > d.nz - 2 || !row_ok) return;
-    const bool right = ((uy + p) & 1) == 0;  // x = xt + 32 (even x) is even-coloured
-    const int x = right ? xt + kSwTX : xt - 1;
-    if (x < 1 || x > d.nx - 2) return;
-    const int h = x & 1, so = (x >> 1) - hx0 + 4;  // 20 (even half) or 3 (odd half)
-    float* E0 = sm.e[se_(p)] + er * kSwW;
-    const float* Em = sm.e[se_(p - 1)] + er * kSwW;
-    const float* Ep = sm.e[se_(p + 1)] + er * kSwW;
-    const float* R = sm.r[sr_(p)] + rr * kSwW;
-    // x+1 / x-1 in the other half: even x -> odd indices so, so-1; odd x -> even indices so+1, so
-    const int op = (1 - h) * kSwHW + (h ? so + 1 : so), om_ = (1 - h) * kSwHW + (h ? so : so - 1);
-    const int me = h * kSwHW + so;
-    unsigned c0 = 0u, cxm = 0u, cym = 0u, czm = 0u;
-    if (!d.uni) {
-      const uint8_t* C0 = sm.c[sc_(p)] + cr * kSwW;
-      const uint8_t* Cm = sm.c[sc_(p - 1)] + cr * kSwW;
-      c0 = C0[me];
-      cxm = C0[om_];
-      cym = C0[me - kSwW];
-      czm = Cm[me];
-    }
-    const int gi = p * d.sz + uy * d.sy + xo(x, hp);
-    float dv;
-    E0[me] = sw_point<kSorMode>(d, sm.tf, om, E0[me], E0[op], E0[om_], E0[me + kSwW], E0[me - kSwW], Ep[me], Em[me],
-                                R[me], c0, cxm, cym, czm, gi, ixm(gi, x, hp), dv);
+  auto even = [&](int p, const float4& rh) {
+    if (role == 2) quad(p, (uy + p) & 1, own_row && p >= z0 && p < z1, rh);
   };
-  auto even = [&](int p) {
-    if (role == 2)
-      quad(p, (uy + p) & 1, own_row && p >= z0 && p < z1);
-    else if (role == 3)
-      halo(p);
+  auto odd = [&](int p, const float4& rh) {
+    if (role == 1) quad(p, (1 + uy + p) & 1, own_row, rh);
   };
-  auto odd = [&](int p) {
-    if (role == 1) quad(p, (1 + uy + p) & 1, own_row);
-  };
-  // store of this thread: one float4 of a tile row half
+  // store of this thread: one float4 of a tile row half; warp w stores rows
+  // 4w .. 4w+3, a quarter warp the same half of rows r and r + 2
   int sso = -1, sgo = 0;
   if (tid < kSwTY * 2 * 4) {
-    const int r = tid >> 3, hh = (tid >> 2) & 1, c = tid & 3, y = yt + r, hi = hx0 + 4 * c;
+    const int pi = (tid >> 2) & 7, r = 4 * (tid >> 5) + ((pi & 1) << 1) + ((pi >> 1) & 1), hh = pi >> 2;
+    const int c = tid & 3, y = yt + r, hi = hx0 + 4 * c;
     if (y < d.ny && hi + 4 <= hp) {
       sso = (r + 2) * kSwW + hh * kSwHW + 4 + 4 * c;
       sgo = y * d.sy + hh * hp + hi;
@@ -664,7 +662,6 @@ __global__ void __launch_bounds__(kSwThreads, 3) k_sweep_t(WL w, const LvlD* __r
   // prologue: what the even points of planes z0-1 .. z0+1 and step z0 read,
   // then the planes of step z0+1
   for (int p = z0 - 2; p <= z0 + 3; p++) load_e(p);
-  for (int p = z0 - 1; p <= z0 + 2; p++) load_r(p);
   for (int p = z0 - 2; p <= z0 + 2; p++) load_c(p);
   cp_async_commit();
   if (!d.uni && tid < 64) {  // face table (read after the barrier below)
@@ -674,25 +671,30 @@ __global__ void __launch_bounds__(kSwThreads, 3) k_sweep_t(WL w, const LvlD* __r
     sm.tf[1][tid] = make_float4(f, g, (a + b) + (c + dd) + (f + g), 0.0f);
   }
   load_e(z0 + 4);
-  load_r(z0 + 3);
   load_c(z0 + 3);
   cp_async_commit();
+  float4 r0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), r1 = r0, r2 = r0;
+  if (role == 2) {
+    r0 = rhs_at(z0 - 1);
+    r1 = rhs_at(z0);
+    r2 = rhs_at(z0 + 1);
+  }
+  float4 rn = rhs_at(role == 1 ? z0 : z0 + 2);  // right-hand side of step z0's update
   cp_async_wait<1>();
   __syncthreads();
-  even(z0 - 1);
-  even(z0);
-  even(z0 + 1);
+  even(z0 - 1, r0);
+  even(z0, r1);
+  even(z0 + 1, r2);
   for (int s = z0; s < z1; s++) {
-    cp_async_wait<1>();  // all groups but the newest: correction planes to s+3, rhs / codes to s+2
+    const float4 rc = rn;
+    cp_async_wait<1>();  // all groups but the newest: correction planes to s+3, codes to s+2
     __syncthreads();
-    if (s + 5 <= z1 + 1) load_e(s + 5);  // the last step reads correction planes to z1+1, rhs / codes to z1
-    if (s + 4 <= z1) {
-      load_r(s + 4);
-      load_c(s + 4);
-    }
+    if (s + 5 <= z1 + 1) load_e(s + 5);  // the last step reads correction planes to z1+1, codes to z1
+    if (s + 4 <= z1) load_c(s + 4);
     cp_async_commit();
-    if (s + 2 <= z1) even(s + 2);
-    odd(s);
+    if (s + 1 < z1) rn = rhs_at(role == 1 ? s + 1 : s + 3);
+    if (s + 2 <= z1) even(s + 2, rc);
+    odd(s, rc);
     if (s > z0) store(s - 1);
   }
   __syncthreads();
@@ -718,7 +720,7 @@ __global__ void k_sor_norm(WL w, const JobD* __restrict__ J, JobState* __restric
   const JobD& d = J[j];
   const bool rel = d.rtol > 0.0;
   const int used = rel ? ((d.nx + 31) >> 5) * ((d.ny + 7) >> 3) * ((d.nz + 7) >> 3)
-                       : ((d.nx + kSwTX - 1) / kSwTX) * ((d.ny + kSwTY - 1) / kSwTY) * ((d.nz + kSwZC0 - 1) / kSwZC0);
+                       : sweep_blocks(0, d.nx, d.ny, d.nz);
   const double* src = rel ? rpart : part;
   double s = 0.0;
   for (int k = threadIdx.x; k < used; k += blockDim.x) s += src[(long long)j * nparts + k];
@@ -1456,7 +1458,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     s.om = 1.0;
     s.status = Y.nlev >= 0 ? kMg : kSor;
     max_res = std::max(max_res, nbricks(J.g));
-    max_sor = std::max(max_sor, cdiv(J.g.nx, kSwTX) * cdiv(J.g.ny, kSwTY) * cdiv(J.g.nz, kSwZC0));  // sweep blocks
+    max_sor = std::max(max_sor, (long long)sweep_blocks(0, J.g.nx, J.g.ny, J.g.nz));
     for (int l = 0; l <= std::max(Y.nlev, 0); l++) {
       const PbGeom& g = Y.lv[l];
       size_t m = padded_n(g);
@@ -1468,7 +1470,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       L.rhs = b + 2 * m;
       L.res = b + 3 * m;
       L.px = pitch(g);
-      L.zc = sweep_chunk(l);
+      L.zc = sweep_zc(l, g.nz);
       if (!J.uniform) {
         L.ex = b + 4 * m;
         L.ey = b + 5 * m;
@@ -1718,7 +1720,14 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     s_sor = lists.add_slot();
     s_snorm = lists.add_slot();
     any_mg = any_sor = false;
-    for (int j = 0; j < nj; j++) {
+    // grids with dielectric maps first: their blocks take longest, and blocks
+    // start in list order, so the short constant-coefficient blocks fill the
+    // tail of each launch
+    std::vector<int> order;
+    for (int pass = 0; pass < 2; pass++)
+      for (int j = 0; j < nj; j++)
+        if (jobs[j].uniform == (pass == 1)) order.push_back(j);
+    for (int j : order) {
       const Lay& Y = lay[j];
       const PbGeom& g = jobs[j].g;
       if (hs[j].status == kMg) {
@@ -1726,7 +1735,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
         maxlev = std::max(maxlev, Y.nlev);
         for (int l = 0; l < Y.nlev; l++) {
           const PbGeom& a = Y.lv[l];
-          lists.add(ls[l].rb, j, cdiv(a.nx, kSwTX) * cdiv(a.ny, kSwTY) * cdiv(a.nz, sweep_chunk(l)));
+          lists.add(ls[l].rb, j, sweep_blocks(l, a.nx, a.ny, a.nz));
           lists.add(ls[l].res, j, nbricks(a));
           lists.add(ls[l].restr, j, nbricks(Y.lv[l + 1]));
           lists.add(ls[l].prol, j, nbricks(a));
@@ -1737,7 +1746,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       } else if (hs[j].status == kSor) {
         any_sor = true;
         lists.add(s_sres, j, nbricks(g));
-        lists.add(s_sor, j, cdiv(g.nx, kSwTX) * cdiv(g.ny, kSwTY) * cdiv(g.nz, kSwZC0));
+        lists.add(s_sor, j, sweep_blocks(0, g.nx, g.ny, g.nz));
         lists.add(s_snorm, j, 1);
       }
     }
