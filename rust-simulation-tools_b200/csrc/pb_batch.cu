@@ -432,8 +432,9 @@ struct SwSmem {
   float e[kSwNE][kSwEY * kSwW];
   uint8_t c[kSwNC][kSwCY * kSwCW];
   // faces of every eps_in / eps_out pattern (bit k set: face k is eps_in;
-  // faces x+, x-, y+, y-, z+, z-): [0] x+, x-, y+, y-; [1] z+, z-, their sum
-  float4 tf[2][64];
+  // faces x+, x-, y+, y-, z+, z-; bit 6: the point's kappa flag):
+  // [0] x+, x-, y+, y-; [1] z+, z-, their sum, the kappa-bar^2 term
+  float4 tf[2][128];
 };
 
 __device__ __forceinline__ void cp_async16(void* s, const void* g) {
@@ -471,6 +472,7 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
   extern __shared__ __align__(16) unsigned char sw_raw[];  // sizeof(SwSmem)
   SwSmem& sm = *reinterpret_cast<SwSmem*>(sw_raw);
   __shared__ double red[32];
+  __shared__ const float* maps[3];  // dielectric maps, read on the rare faces that cross the surface
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != (kSorMode ? kSor : kMg)) return;
   const Lv d = lv_load(L, j, lvl);
@@ -525,24 +527,28 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
   // s+2.  Quads 0..3 of a row cover the tile's 16 points of one colour; an
   // even row's quad 4 covers its x-halo point (x = xt+32 in the even half or
   // x = xt-1 in the odd half, whichever is even-coloured) and three more
-  // points that are computed but neither stored nor read.  A thread of quads
-  // 0..3 takes quad (lane & 3) of row 2 ((lane >> 2) & 3) + (lane >> 4) among
-  // its warp's eight rows.
-  const int lane = tid & 31, lrow = 2 * ((lane >> 2) & 3) + (lane >> 4);
+  // points that are computed but neither stored nor read.  Warps 0 and 1 take
+  // the odd quads of rows yt + w + 2i, warps 2 and 3 the even quads of rows
+  // yt - 1 + (w - 2) + 2i (i = lane >> 2, quad lane & 3): the rows of such a
+  // warp share their colour parity, so the half that holds a colour is the
+  // same across the warp, and a quarter warp's rows r and r + 2 start 16
+  // banks apart.  Warp 4 takes the even quads 0..3 of rows yt+15 and yt+16
+  // and the quads 4 of all 18 rows.
+  const int lane = tid & 31, wp = tid >> 5;
   int role = 0, uy = 0, uq = lane & 3;
-  if (tid < 64) {
+  if (wp < 2) {
     role = 1;
-    uy = yt + 8 * (tid >> 5) + lrow;
-  } else if (tid < 128) {
+    uy = yt + wp + 2 * (lane >> 2);
+  } else if (wp < 4) {
     role = 2;
-    uy = yt - 1 + 8 * ((tid - 64) >> 5) + lrow;
-  } else if (tid < 136) {
+    uy = yt - 1 + (wp - 2) + 2 * (lane >> 2);
+  } else if (lane < 8) {
     role = 2;
-    uy = yt + 15 + ((tid - 128) >> 2);
-  } else if (tid < 154) {
+    uy = yt + 15 + (lane >> 2);
+  } else if (lane < 26) {
     role = 2;
-    uy = yt - 1 + (tid - 136);
     uq = 4;
+    uy = lane < 17 ? yt - 1 + 2 * (lane - 8) : yt + 2 * (lane - 17);
   }
   const bool row_act = role != 0 && uy >= 1 && uy <= d.ny - 2;  // interior row
   const bool own_row = uq < 4 && uy >= yt && uy < yt + kSwTY;
@@ -558,7 +564,7 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
     return __ldg(reinterpret_cast<const float4*>(d.rhs + (long long)d.sz * p + uy * d.sy + h * hp + hi0));
   };
   // the four points of a quad: half h, half-indices hi0 + k
-  auto quad = [&](int p, int h, bool own, const float4& rh) {
+  auto quad = [&](int h, int p, bool own, const float4& rh) {
     const int so = qso(h), hi0 = hx0 - 4 + so;
     if (!row_act || p < 1 || p > d.nz - 2 || hi0 < 0 || hi0 >= hp) return;
     float* E0 = sm.e[se_(p)] + er * kSwW;
@@ -605,31 +611,32 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
       const unsigned czm = *(const unsigned*)&Cm[h * kSwHW + so];
       const unsigned w1 = *(const unsigned*)&C0[(1 - h) * kSwHW + so];
       const unsigned cxm = h ? w1 : __funnelshift_r(*(const unsigned*)&C0[(1 - h) * kSwHW + so - 4], w1, 24);
-      // per point (one byte each): the eps_in bits of its six faces, an index
-      // into tf, and whether a face crosses the surface (2-bit face code 2:
-      // the dielectric comes from the maps)
+      // per point (one byte each): the eps_in bits of its six faces and its
+      // kappa flag, an index into tf, and whether a face crosses the surface
+      // (2-bit face code 2: the dielectric comes from the maps)
       const unsigned pat =
-          (c0 & 0x15151515u) | (((cxm & 0x01010101u) | (cym & 0x04040404u) | (czm & 0x10101010u)) << 1);
+          (c0 & 0x55555555u) | (((cxm & 0x01010101u) | (cym & 0x04040404u) | (czm & 0x10101010u)) << 1);
       const unsigned crs = (c0 & 0x2A2A2A2Au) | (cxm & 0x02020202u) | (cym & 0x08080808u) | (czm & 0x20202020u);
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         if (k > kmax || (k == 0 && !k0)) continue;
-        const unsigned pk = (pat >> (8 * k)) & 63u;
+        const unsigned pk = (pat >> (8 * k)) & 127u;
         const float4 u = sm.tf[0][pk], v = sm.tf[1][pk];
-        float a = u.x, b = u.y, c = u.z, dd = u.w, f = v.x, g = v.y, sum = v.z;
+        float a = u.x, b = u.y, c = u.z, dd = u.w, f = v.x, g = v.y, sum = v.z;  // v.w: kappa-bar^2 term
         if ((crs >> (8 * k)) & 0xFFu) {
           const int gi = gb + k;
           const unsigned q0 = c0 >> (8 * k), qx = cxm >> (8 * k), qy = cym >> (8 * k), qz = czm >> (8 * k);
-          if (q0 & 2u) a = d.ex[gi];
-          if (qx & 2u) b = d.ex[ixm(gi, lo + 2 * k, hp)];
-          if (q0 & 8u) c = d.ey[gi];
-          if (qy & 8u) dd = d.ey[gi - d.sy];
-          if (q0 & 32u) f = d.ez[gi];
-          if (qz & 32u) g = d.ez[gi - d.sz];
+          const float *__restrict__ mx = maps[0], *__restrict__ my = maps[1], *__restrict__ mz = maps[2];
+          if (q0 & 2u) a = mx[gi];
+          if (qx & 2u) b = mx[ixm(gi, lo + 2 * k, hp)];
+          if (q0 & 8u) c = my[gi];
+          if (qy & 8u) dd = my[gi - d.sy];
+          if (q0 & 32u) f = mz[gi];
+          if (qz & 32u) g = mz[gi - d.sz];
           sum = (a + b) + (c + dd) + (f + g);
         }
         const float ns = ((a * vxp[k] + b * vxm[k]) + (c * vyp[k] + dd * vym[k]) + (f * vzp[k] + g * vzm[k])) * d.ih;
-        const float dg = fmaf(sum, d.ih, ((c0 >> (8 * k)) & 64u) ? d.kb : 0.0f);
+        const float dg = fmaf(sum, d.ih, v.w);
         const float gs = kSorMode ? (ns + vr[k]) / dg : __fdividef(ns + vr[k], dg);
         const float dv = gs - o[k];
         o[k] = o[k] + om * dv;
@@ -639,10 +646,10 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
     *(float4*)&E0[h * kSwHW + so] = make_float4(o[0], o[1], o[2], o[3]);
   };
   auto even = [&](int p, const float4& rh) {
-    if (role == 2) quad(p, (uy + p) & 1, own_row && p >= z0 && p < z1, rh);
+    if (role == 2) quad((uy + p) & 1, p, own_row && p >= z0 && p < z1, rh);
   };
   auto odd = [&](int p, const float4& rh) {
-    if (role == 1) quad(p, (1 + uy + p) & 1, own_row, rh);
+    if (role == 1) quad((1 + uy + p) & 1, p, own_row, rh);
   };
   // store of this thread: one float4 of a tile row half; warp w stores rows
   // 4w .. 4w+3, a quarter warp the same half of rows r and r + 2
@@ -664,11 +671,16 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
   for (int p = z0 - 2; p <= z0 + 3; p++) load_e(p);
   for (int p = z0 - 2; p <= z0 + 2; p++) load_c(p);
   cp_async_commit();
-  if (!d.uni && tid < 64) {  // face table (read after the barrier below)
+  if (tid == 0) {
+    maps[0] = d.ex;
+    maps[1] = d.ey;
+    maps[2] = d.ez;
+  }
+  if (!d.uni && tid < 128) {  // face table (read after the barrier below)
     const float a = (tid & 1) ? d.fin : d.fout, b = (tid & 2) ? d.fin : d.fout, c = (tid & 4) ? d.fin : d.fout,
                 dd = (tid & 8) ? d.fin : d.fout, f = (tid & 16) ? d.fin : d.fout, g = (tid & 32) ? d.fin : d.fout;
     sm.tf[0][tid] = make_float4(a, b, c, dd);
-    sm.tf[1][tid] = make_float4(f, g, (a + b) + (c + dd) + (f + g), 0.0f);
+    sm.tf[1][tid] = make_float4(f, g, (a + b) + (c + dd) + (f + g), (tid & 64) ? d.kb : 0.0f);
   }
   load_e(z0 + 4);
   load_c(z0 + 3);
