@@ -301,32 +301,45 @@ __global__ void __launch_bounds__(256, 4) k_upres64(WL w, const JobD* __restrict
     const bool inxy = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
     int i = x + sy * y + sz * z0, ci = xo(x, hp) + cy * y + cz * z0;  // FP64 and split FP32 / code indices
     const int dxp = ixp(0, x, hp), dxm = ixm(0, x, hp);              // offsets of x + 1, x - 1
+    // phi + e of the column at z - 1 and z, and the code at z - 1, carried
+    // along z: each value is formed once, the loads of the eight points are
+    // independent
+    double vm = 0.0, v0 = p[i] + (double)e0[ci];
+    unsigned cm = 0u;
+    if (z0 >= 1) {
+      vm = p[i - sz] + (double)e0[ci - cz];
+      if (inxy) cm = cd[ci - cz];
+    }
 #pragma unroll 1
     for (int k = 0; k < 8; k++, i += sz, ci += cz) {
       const int z = z0 + k;
       if (z >= nz) break;
-      const double v = p[i] + (double)e0[ci];
-      q[i] = v;
-      if (!inxy || z < 1 || z > nz - 2) continue;
-      const double vxp = p[i + 1] + (double)e0[ci + dxp], vxm = p[i - 1] + (double)e0[ci + dxm],
-                   vyp = p[i + sy] + (double)e0[ci + cy], vym = p[i - sy] + (double)e0[ci - cy],
-                   vzp = p[i + sz] + (double)e0[ci + cz], vzm = p[i - sz] + (double)e0[ci - cz];
-      const unsigned c0 = cd[ci];
-      double ns, dg;
-      if (uni) {
-        ns = wt * ((vxp + vxm) + (vyp + vym) + (vzp + vzm));
-        dg = 6.0 * wt;
-      } else {
-        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci + dxm] & 3u, ex, i - 1, din, dout),
-               c = face((c0 >> 2) & 3u, ey, i, din, dout), dd = face((cd[ci - cy] >> 2) & 3u, ey, i - sy, din, dout),
-               f = face((c0 >> 4) & 3u, ez, i, din, dout), g = face((cd[ci - cz] >> 4) & 3u, ez, i - sz, din, dout);
-        ns = (a * vxp + b * vxm) * ih + (c * vyp + dd * vym) * ih + (f * vzp + g * vzm) * ih;
-        dg = (a + b) * ih + (c + dd) * ih + (f + g) * ih + ((c0 & 64u) ? dkb : 0.0);
+      const double vp = z + 1 < nz ? p[i + sz] + (double)e0[ci + cz] : 0.0;
+      q[i] = v0;
+      const unsigned c0 = inxy ? (unsigned)cd[ci] : 0u;
+      if (inxy && z >= 1 && z <= nz - 2) {
+        const double vxp = p[i + 1] + (double)e0[ci + dxp], vxm = p[i - 1] + (double)e0[ci + dxm],
+                     vyp = p[i + sy] + (double)e0[ci + cy], vym = p[i - sy] + (double)e0[ci - cy];
+        double ns, dg;
+        if (uni) {
+          ns = wt * ((vxp + vxm) + (vyp + vym) + (vp + vm));
+          dg = 6.0 * wt;
+        } else {
+          double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci + dxm] & 3u, ex, i - 1, din, dout),
+                 c = face((c0 >> 2) & 3u, ey, i, din, dout),
+                 dd = face((cd[ci - cy] >> 2) & 3u, ey, i - sy, din, dout), f = face((c0 >> 4) & 3u, ez, i, din, dout),
+                 g = face((cm >> 4) & 3u, ez, i - sz, din, dout);
+          ns = (a * vxp + b * vxm) * ih + (c * vyp + dd * vym) * ih + (f * vp + g * vm) * ih;
+          dg = (a + b) * ih + (c + dd) * ih + (f + g) * ih + ((c0 & 64u) ? dkb : 0.0);
+        }
+        double rq = (c0 & 128u) ? rho[i] : 0.0;
+        double r = kFourPiEcB * rq + ns - dg * v0;
+        rhs0[ci] = (float)r;
+        acc += r * r;
       }
-      double rq = (c0 & 128u) ? rho[i] : 0.0;
-      double r = kFourPiEcB * rq + ns - dg * v;
-      rhs0[ci] = (float)r;
-      acc += r * r;
+      cm = c0;
+      vm = v0;
+      v0 = vp;
     }
   }
   double t = block_sum(acc, sh);
