@@ -138,7 +138,7 @@ struct Lv {
   float *__restrict__ e, *__restrict__ e2, *__restrict__ rhs, *__restrict__ res;
   const float *__restrict__ ex, *__restrict__ ey, *__restrict__ ez, *__restrict__ k2;
   const uint8_t* __restrict__ cd;
-  int nx, ny, nz, sy, sz, zc, hp;
+  int nx, ny, nz, sy, sz, zc;
   bool uni;
   float ih, om, w6, fin, fout, kb;
 };
@@ -159,7 +159,6 @@ __device__ __forceinline__ Lv lv_load(const LvlD* __restrict__ L, int j, int lvl
   v.nz = d.nz;
   v.sy = d.px;
   v.sz = d.px * d.ny;
-  v.hp = d.px >> 1;
   v.zc = d.zc;
   v.uni = d.uniform != 0;
   v.ih = d.ih;
@@ -177,14 +176,6 @@ __device__ __forceinline__ T face(unsigned c, const T* __restrict__ m, int i, T 
   return c == 0u ? eout : (c == 1u ? ein : m[i]);
 }
 
-// Split rows: every FP32 level array and the stencil codes store a row as its
-// even-x points followed, half a row pitch later, by its odd-x points, so the
-// points of one colour of a red-black sweep are contiguous in a row and move
-// as 16-byte vectors.  hp is the half pitch (elements).
-__device__ __forceinline__ int xo(int x, int hp) { return (x & 1) * hp + (x >> 1); }
-__device__ __forceinline__ int ixp(int i, int x, int hp) { return (x & 1) ? i - hp + 1 : i + hp; }  // x + 1
-__device__ __forceinline__ int ixm(int i, int x, int hp) { return (x & 1) ? i - hp : i + hp - 1; }  // x - 1
-
 // Brick of 32 x 8 x 8 points for a 256-thread block: thread (lane, warp) owns
 // the column (x, y) = (x0 + lane, y0 + warp) over the brick's 8 z planes, so
 // the index arithmetic is done once per block and the 8 points of a column
@@ -199,19 +190,19 @@ __device__ __forceinline__ void brick_col(int lb, int nx, int ny, int& x, int& y
 
 // FP32 7-point stencil of pb_solver.rs:250-317: ns = sum of eps-weighted
 // neighbours, dg = diagonal.
-__device__ __forceinline__ void st32(const Lv& d, const float* __restrict__ e, int x, int i, float& ns, float& dg) {
-  const int sy = d.sy, sz = d.sz, ip = ixp(i, x, d.hp), im = ixm(i, x, d.hp);
+__device__ __forceinline__ void st32(const Lv& d, const float* __restrict__ e, int i, float& ns, float& dg) {
+  const int sy = d.sy, sz = d.sz;
   if (d.uni) {
-    ns = d.w6 * ((e[ip] + e[im]) + (e[i + sy] + e[i - sy]) + (e[i + sz] + e[i - sz]));
+    ns = d.w6 * ((e[i + 1] + e[i - 1]) + (e[i + sy] + e[i - sy]) + (e[i + sz] + e[i - sz]));
     dg = 6.0f * d.w6;
   } else {
     const unsigned c0 = d.cd[i];
-    float a = face(c0 & 3u, d.ex, i, d.fin, d.fout), b = face(d.cd[im] & 3u, d.ex, im, d.fin, d.fout),
+    float a = face(c0 & 3u, d.ex, i, d.fin, d.fout), b = face(d.cd[i - 1] & 3u, d.ex, i - 1, d.fin, d.fout),
           c = face((c0 >> 2) & 3u, d.ey, i, d.fin, d.fout),
           dd = face((d.cd[i - sy] >> 2) & 3u, d.ey, i - sy, d.fin, d.fout),
           f = face((c0 >> 4) & 3u, d.ez, i, d.fin, d.fout),
           g = face((d.cd[i - sz] >> 4) & 3u, d.ez, i - sz, d.fin, d.fout);
-    ns = ((a * e[ip] + b * e[im]) + (c * e[i + sy] + dd * e[i - sy]) + (f * e[i + sz] + g * e[i - sz])) * d.ih;
+    ns = ((a * e[i + 1] + b * e[i - 1]) + (c * e[i + sy] + dd * e[i - sy]) + (f * e[i + sz] + g * e[i - sz])) * d.ih;
     dg = ((a + b) + (c + dd) + (f + g)) * d.ih + ((c0 & 64u) ? d.kb : 0.0f);
   }
 }
@@ -234,13 +225,12 @@ __global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__
   const double din = d.din, dout = d.dout, dkb = d.dkb;
   const bool uni = d.uniform != 0;
   const double ih = d.ih, wt = d.eps * d.ih;
-  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny, hp = d.px >> 1;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny;
   int x, y, z0;
   brick_col(lb, nx, ny, x, y, z0);
   double acc = 0.0;
   if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
-    int i = x + sy * y + sz * z0, ci = xo(x, hp) + cy * y + cz * z0;  // FP64 and split FP32 / code indices
-    const int dxm = ixm(0, x, hp);                                     // code offset of x - 1
+    int i = x + sy * y + sz * z0, ci = x + cy * y + cz * z0;  // FP64 and padded FP32 / code indices
 #pragma unroll
     for (int k = 0; k < 8; k++, i += sz, ci += cz) {
       int z = z0 + k;
@@ -251,7 +241,7 @@ __global__ void __launch_bounds__(256, 4) k_res64(WL w, const JobD* __restrict__
         ns = wt * ((p[i + 1] + p[i - 1]) + (p[i + sy] + p[i - sy]) + (p[i + sz] + p[i - sz]));
         dg = 6.0 * wt;
       } else {
-        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci + dxm] & 3u, ex, i - 1, din, dout),
+        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci - 1] & 3u, ex, i - 1, din, dout),
                c = face((c0 >> 2) & 3u, ey, i, din, dout), dd = face((cd[ci - cy] >> 2) & 3u, ey, i - sy, din, dout),
                f = face((c0 >> 4) & 3u, ez, i, din, dout), g = face((cd[ci - cz] >> 4) & 3u, ez, i - sz, din, dout);
         ns = (a * p[i + 1] + b * p[i - 1]) * ih + (c * p[i + sy] + dd * p[i - sy]) * ih +
@@ -293,53 +283,39 @@ __global__ void __launch_bounds__(256, 4) k_upres64(WL w, const JobD* __restrict
   const double din = d.din, dout = d.dout, dkb = d.dkb;
   const bool uni = d.uniform != 0;
   const double ih = d.ih, wt = d.eps * d.ih;
-  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny, hp = d.px >> 1;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, sy = nx, sz = nx * ny, cy = d.px, cz = d.px * ny;
   int x, y, z0;
   brick_col(lb, nx, ny, x, y, z0);
   double acc = 0.0;
   if (x < nx && y < ny) {
     const bool inxy = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
-    int i = x + sy * y + sz * z0, ci = xo(x, hp) + cy * y + cz * z0;  // FP64 and split FP32 / code indices
-    const int dxp = ixp(0, x, hp), dxm = ixm(0, x, hp);              // offsets of x + 1, x - 1
-    // phi + e of the column at z - 1 and z, and the code at z - 1, carried
-    // along z: each value is formed once, the loads of the eight points are
-    // independent
-    double vm = 0.0, v0 = p[i] + (double)e0[ci];
-    unsigned cm = 0u;
-    if (z0 >= 1) {
-      vm = p[i - sz] + (double)e0[ci - cz];
-      if (inxy) cm = cd[ci - cz];
-    }
+    int i = x + sy * y + sz * z0, ci = x + cy * y + cz * z0;  // FP64 and padded FP32 / code indices
 #pragma unroll 1
     for (int k = 0; k < 8; k++, i += sz, ci += cz) {
       const int z = z0 + k;
       if (z >= nz) break;
-      const double vp = z + 1 < nz ? p[i + sz] + (double)e0[ci + cz] : 0.0;
-      q[i] = v0;
-      const unsigned c0 = inxy ? (unsigned)cd[ci] : 0u;
-      if (inxy && z >= 1 && z <= nz - 2) {
-        const double vxp = p[i + 1] + (double)e0[ci + dxp], vxm = p[i - 1] + (double)e0[ci + dxm],
-                     vyp = p[i + sy] + (double)e0[ci + cy], vym = p[i - sy] + (double)e0[ci - cy];
-        double ns, dg;
-        if (uni) {
-          ns = wt * ((vxp + vxm) + (vyp + vym) + (vp + vm));
-          dg = 6.0 * wt;
-        } else {
-          double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci + dxm] & 3u, ex, i - 1, din, dout),
-                 c = face((c0 >> 2) & 3u, ey, i, din, dout),
-                 dd = face((cd[ci - cy] >> 2) & 3u, ey, i - sy, din, dout), f = face((c0 >> 4) & 3u, ez, i, din, dout),
-                 g = face((cm >> 4) & 3u, ez, i - sz, din, dout);
-          ns = (a * vxp + b * vxm) * ih + (c * vyp + dd * vym) * ih + (f * vp + g * vm) * ih;
-          dg = (a + b) * ih + (c + dd) * ih + (f + g) * ih + ((c0 & 64u) ? dkb : 0.0);
-        }
-        double rq = (c0 & 128u) ? rho[i] : 0.0;
-        double r = kFourPiEcB * rq + ns - dg * v0;
-        rhs0[ci] = (float)r;
-        acc += r * r;
+      const double v = p[i] + (double)e0[ci];
+      q[i] = v;
+      if (!inxy || z < 1 || z > nz - 2) continue;
+      const double vxp = p[i + 1] + (double)e0[ci + 1], vxm = p[i - 1] + (double)e0[ci - 1],
+                   vyp = p[i + sy] + (double)e0[ci + cy], vym = p[i - sy] + (double)e0[ci - cy],
+                   vzp = p[i + sz] + (double)e0[ci + cz], vzm = p[i - sz] + (double)e0[ci - cz];
+      const unsigned c0 = cd[ci];
+      double ns, dg;
+      if (uni) {
+        ns = wt * ((vxp + vxm) + (vyp + vym) + (vzp + vzm));
+        dg = 6.0 * wt;
+      } else {
+        double a = face(c0 & 3u, ex, i, din, dout), b = face(cd[ci - 1] & 3u, ex, i - 1, din, dout),
+               c = face((c0 >> 2) & 3u, ey, i, din, dout), dd = face((cd[ci - cy] >> 2) & 3u, ey, i - sy, din, dout),
+               f = face((c0 >> 4) & 3u, ez, i, din, dout), g = face((cd[ci - cz] >> 4) & 3u, ez, i - sz, din, dout);
+        ns = (a * vxp + b * vxm) * ih + (c * vyp + dd * vym) * ih + (f * vzp + g * vzm) * ih;
+        dg = (a + b) * ih + (c + dd) * ih + (f + g) * ih + ((c0 & 64u) ? dkb : 0.0);
       }
-      cm = c0;
-      vm = v0;
-      v0 = vp;
+      double rq = (c0 & 128u) ? rho[i] : 0.0;
+      double r = kFourPiEcB * rq + ns - dg * v;
+      rhs0[ci] = (float)r;
+      acc += r * r;
     }
   }
   double t = block_sum(acc, sh);
@@ -391,63 +367,46 @@ __global__ void k_norm(WL w, const JobD* __restrict__ J, JobState* __restrict__ 
 // One full red-black sweep on one level (pb_solver.rs:250-317): every even
 // point (x + y + z even) from its odd neighbours, then every odd point from
 // the updated even ones, each point with the arithmetic of the
-// single-colour update.  A block owns an x-y tile of 32 x 16 points and
-// marches a chunk of z planes.  Planes of the correction (with a two-row
-// halo) and of the stencil codes stream into shared-memory rings with
-// cp.async, two steps ahead of their use; the right-hand side, which one
-// thread reads per point, streams through registers one step ahead.  Step s
+// single-colour update.  A block owns an x-y tile of kSwTX x kSwTY points and
+// marches a chunk of z planes.  Planes of the correction (with a two-point
+// halo), of the right-hand side and of the stencil codes stream into
+// shared-memory rings with cp.async, two steps ahead of their use.  Step s
 // updates, in one phase between barriers, the even points of plane s+2 over
 // the tile and a one-point halo, the odd points of plane s (whose even
 // neighbours in planes s-1 .. s+1 are already updated) and writes plane s-1
 // out.  Halo values are recomputed by each tile that needs them, so the sweep
 // reads `src` and writes the whole grid, boundary values copied, into `dst`:
-// no block reads what another block writes.
-//
-// Rows are split by x parity in global and shared memory (see xo), so the
-// points of one colour in a row are contiguous: a thread updates four of
-// them with 16-byte loads of the point values, of each of the y / z
-// neighbour rows, of the right-hand side and of the other half (the x
-// neighbours), and 4-byte loads of four stencil codes.  160 threads: 64
-// update four odd points of plane s each (16 rows x 4 quads), 90 four even
-// points of plane s+2 (18 rows: the tile and a y halo row on each side; five
-// quads a row, the fifth for the row's x-halo point, x = xt-1 or xt+32,
-// whichever is even-coloured).  The quads 0..3 of a quarter warp lie in rows
-// r and r + 2, whose points have the same colour parity; with shared rows of
-// 56 floats those rows start 16 banks apart, so each 16-byte load of a
-// quarter warp touches every bank once.
-constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 160, kSwZC0 = 24, kSwZC1 = 16;
+// no block reads what another block writes.  Each thread's points, copy
+// chunks and store are fixed for the whole march (only the colour parity
+// alternates with the plane), so the per-step index work is a few adds; a
+// half-warp covers 16 points of one colour in a row and the next half-warp
+// the next row (opposite parity), so the shared loads are free of bank
+// conflicts; ring depths are powers of two.
 // z planes per block: long marches on the finest level, short ones on the
-// coarse levels (few tiles per grid there, so more chunks keep the SMs busy);
-// a grid's planes are dealt evenly over its chunks
-__host__ __device__ inline int sweep_zc(int lvl, int nz) {
-  const int base = lvl == 0 ? kSwZC0 : (lvl == 1 ? kSwZC1 : 8);
-  const int k = nz > base ? (nz + base - 1) / base : 1;
-  return nz > 0 ? (nz + k - 1) / k : 1;
-}
-__host__ __device__ inline int sweep_blocks(int lvl, int nx, int ny, int nz) {
-  const int zc = sweep_zc(lvl, nz);
-  return ((nx + kSwTX - 1) / kSwTX) * ((ny + kSwTY - 1) / kSwTY) * ((nz + zc - 1) / zc);
-}
-constexpr int kSwHW = 24;         // shared half-row: half-indices [hx0-4, hx0+20), hx0 = xt/2
-constexpr int kSwW = 56;          // shared correction row: even half, odd half, 8 floats of padding
-constexpr int kSwCW = 2 * kSwHW;  // shared code row (bytes): even half, odd half
+// coarse levels (few tiles per grid there, so more chunks keep the SMs busy)
+constexpr int kSwTX = 32, kSwTY = 16, kSwThreads = 288, kSwZC0 = 48, kSwZC1 = 16;
+int sweep_chunk(int lvl) { return lvl == 0 ? kSwZC0 : (lvl == 1 ? kSwZC1 : 8); }
+constexpr int kSwW = kSwTX + 8;   // shared row: x in [xt-4, xt+TX+4), 16-byte chunks
 constexpr int kSwEY = kSwTY + 4;  // correction rows: y in [yt-2, yt+TY+2)
+constexpr int kSwRY = kSwTY + 2;  // right-hand-side rows: y in [yt-1, yt+TY+1)
 constexpr int kSwCY = kSwTY + 3;  // code rows: y in [yt-2, yt+TY+1)
-constexpr int kSwNE = 8, kSwNC = 8;   // ring depths in planes (slot = plane & (depth - 1))
-constexpr int kSwChunks = kSwHW / 4;  // 16-byte (or 4-code) chunks per half-row
-static_assert(kSwTX == 32 && kSwTY == 16, "thread roles of the sweep");
-static_assert((2 * kSwW) % 32 == 16 && kSwW >= 2 * kSwHW, "rows r and r + 2 start 16 banks apart");
-static_assert(kSwEY * 2 * kSwChunks <= 2 * kSwThreads && kSwCY * 2 * kSwChunks <= 2 * kSwThreads &&
-                  kSwTY * 2 * 4 <= kSwThreads,
-              "two copy chunks and one store per thread and plane");
+constexpr int kSwNE = 8, kSwNR = 8, kSwNC = 8;  // ring depths in planes (slot = plane & (depth - 1))
+// first point of a thread: even points of plane s+2 inside the tile's x range, 16 per row, rows yt-1 .. yt+TY;
+// second point: odd points of plane s (threads < TY*16), then the even points of plane s+2 on the
+// x halo (one per row: x = xt-1 or xt+TX)
+static_assert(kSwTX == 32 && (kSwTY + 2) * 16 == kSwThreads && kSwTY * 16 + kSwTY + 2 <= kSwThreads,
+              "point assignment of the sweep");
+static_assert(kSwEY * (kSwW / 4) <= kSwThreads && kSwRY * (kSwW / 4) <= kSwThreads &&
+                  kSwCY * (kSwW / 4) <= kSwThreads && kSwTY * (kSwTX / 4) <= kSwThreads,
+              "one copy chunk and one store per thread and plane");
 
 struct SwSmem {
   float e[kSwNE][kSwEY * kSwW];
-  uint8_t c[kSwNC][kSwCY * kSwCW];
+  float r[kSwNR][kSwRY * kSwW];
+  uint8_t c[kSwNC][kSwCY * kSwW];
   // faces of every eps_in / eps_out pattern (bit k set: face k is eps_in;
-  // faces x+, x-, y+, y-, z+, z-; bit 6: the point's kappa flag):
-  // [0] x+, x-, y+, y-; [1] z+, z-, their sum, the kappa-bar^2 term
-  float4 tf[2][128];
+  // faces x+, x-, y+, y-, z+, z-): [0] x+, x-, y+, y-; [1] z+, z-, their sum
+  float4 tf[2][64];
 };
 
 __device__ __forceinline__ void cp_async16(void* s, const void* g) {
@@ -464,15 +423,47 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// The update of one interior point (pb_solver.rs:250-317), in quad() below:
-// ns = sum over the six faces of eps_face * neighbour / h^2, dg = sum of
-// eps_face / h^2 (+ kappa-bar^2 where the point's kappa flag is set),
-// gs = (ns + rhs) / dg, new = old + omega (gs - old).  A face dielectric is
-// eps_out, eps_in or, where the face crosses the surface, the map value; the
-// first two come from tf by the point's six eps_in bits and the map faces
-// replace them.  Multigrid smoothing divides with the fast reciprocal; the
-// SOR fallback (pb_solver.rs:373-447) with the exact division, as a plain
-// sweep does.
+// Update of one interior point: off is its offset in the shared planes (the
+// right-hand-side planes start one row later), gi its padded global index
+// (for the map values of faces that cross the surface).  Returns gs - old.
+// Multigrid smoothing divides with the fast reciprocal; the SOR fallback
+// (pb_solver.rs:373-447) with the exact division, as a plain sweep does.
+template <bool kExact>
+__device__ __forceinline__ float sw_update(const Lv& d, const float4 (*__restrict__ tf)[64], float om,
+                                           float* __restrict__ E0, const float* __restrict__ Em,
+                                           const float* __restrict__ Ep, const float* __restrict__ R,
+                                           const uint8_t* __restrict__ C0, const uint8_t* __restrict__ Cm, int off,
+                                           int gi) {
+  float* ec = E0 + off;
+  const float xm = ec[-1], xp = ec[1], ym = ec[-kSwW], yp = ec[kSwW], zm = Em[off], zp = Ep[off], old = ec[0];
+  const float rhs = R[off - kSwW];
+  float ns, dg;
+  if (d.uni) {
+    ns = d.w6 * ((xp + xm) + (yp + ym) + (zp + zm));
+    dg = 6.0f * d.w6;
+  } else {
+    const unsigned c0 = C0[off], cxm = C0[off - 1], cym = C0[off - kSwW], czm = Cm[off];
+    const float k2 = (c0 & 64u) ? d.kb : 0.0f;
+    if (((c0 & 0x2Au) | (cxm & 0x2u) | (cym & 0x8u) | (czm & 0x20u)) == 0u) {  // no face crosses the surface
+      const unsigned pat = (c0 & 0x15u) | ((cxm & 0x1u) << 1) | ((cym & 0x4u) << 1) | ((czm & 0x10u) << 1);
+      const float4 u = tf[0][pat], v = tf[1][pat];
+      ns = ((u.x * xp + u.y * xm) + (u.z * yp + u.w * ym) + (v.x * zp + v.y * zm)) * d.ih;
+      dg = fmaf(v.z, d.ih, k2);
+    } else {
+      const float a = face(c0 & 3u, d.ex, gi, d.fin, d.fout), b = face(cxm & 3u, d.ex, gi - 1, d.fin, d.fout),
+                  c = face((c0 >> 2) & 3u, d.ey, gi, d.fin, d.fout),
+                  dd = face((cym >> 2) & 3u, d.ey, gi - d.sy, d.fin, d.fout),
+                  f = face((c0 >> 4) & 3u, d.ez, gi, d.fin, d.fout),
+                  g = face((czm >> 4) & 3u, d.ez, gi - d.sz, d.fin, d.fout);
+      ns = ((a * xp + b * xm) + (c * yp + dd * ym) + (f * zp + g * zm)) * d.ih;
+      dg = fmaf((a + b) + (c + dd) + (f + g), d.ih, k2);
+    }
+  }
+  const float gs = kExact ? (ns + rhs) / dg : __fdividef(ns + rhs, dg);
+  const float dv = gs - old;
+  ec[0] = old + om * dv;
+  return dv;
+}
 
 // kSorMode: one sweep of the SOR fallback on the finest level's correction
 // equation from e = 0 (zero_src), with the grid's Chebyshev omega, and per
@@ -482,10 +473,9 @@ template <bool kSorMode>
 __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __restrict__ L, int lvl,
                                                         const JobState* __restrict__ S, int flip, int zero_src,
                                                         double* __restrict__ part, int nparts) {
-  extern __shared__ __align__(16) unsigned char sw_raw[];  // sizeof(SwSmem)
+  extern __shared__ __align__(16) unsigned char sw_raw[];  // sizeof(SwSmem), above the 48 KB static limit
   SwSmem& sm = *reinterpret_cast<SwSmem*>(sw_raw);
   __shared__ double red[32];
-  __shared__ const float* maps[3];  // dielectric maps, read on the rare faces that cross the surface
   int lb, j = wl_job(w, blockIdx.x, lb);
   if (S[j].status != (kSorMode ? kSor : kMg)) return;
   const Lv d = lv_load(L, j, lvl);
@@ -495,186 +485,108 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
   float* __restrict__ dst = flip ? d.e : d.e2;
   const int ntx = (d.nx + kSwTX - 1) / kSwTX, nty = (d.ny + kSwTY - 1) / kSwTY;
   const int bx = lb % ntx, q = lb / ntx, by = q % nty, bz = q / nty;
-  const int xt = bx * kSwTX, yt = by * kSwTY, hx0 = xt >> 1, hp = d.hp;
+  const int xt = bx * kSwTX, yt = by * kSwTY;
   const int z0 = bz * d.zc, z1 = min(z0 + d.zc, d.nz);
   const int tid = threadIdx.x;
 
-  // copy chunks of this thread: k-th chunk of a plane is (row, half, c);
-  // shared offset (row stride `stride`) and global offset within a plane, -1: none
-  auto chunk = [&](int k, int rows, int y0, int stride, int& so, int& go) {
+  // copy chunks of this thread (shared offset, global offset within a plane; -1: none)
+  auto chunk = [&](int rows, int y0, int& so, int& go) {
     so = go = -1;
-    if (k >= rows * 2 * kSwChunks) return;
-    const int r = k / (2 * kSwChunks), hh = (k / kSwChunks) & 1, c = k % kSwChunks, y = y0 + r;
-    const int hi = hx0 - 4 + 4 * c;  // first half-index of the chunk
-    if (y < 0 || y >= d.ny || hi < 0 || hi + 4 > hp) return;
-    so = r * stride + hh * kSwHW + 4 * c;
-    go = y * d.sy + hh * hp + hi;
+    if (tid >= rows * (kSwW / 4)) return;
+    const int r = tid / (kSwW / 4), c = tid % (kSwW / 4), y = y0 + r, x = xt - 4 + 4 * c;
+    if (y < 0 || y >= d.ny || x < 0 || x >= d.sy) return;
+    so = r * kSwW + 4 * c;
+    go = x + d.sy * y;
   };
-  int eso[2], ego[2], cso[2], cgo[2];
-#pragma unroll
-  for (int u = 0; u < 2; u++) {
-    chunk(tid + u * kSwThreads, kSwEY, yt - 2, kSwW, eso[u], ego[u]);
-    chunk(tid + u * kSwThreads, kSwCY, yt - 2, kSwCW, cso[u], cgo[u]);
-    if (d.uni) cso[u] = cgo[u] = -1;  // constant-coefficient grids read no codes (coarse levels have none)
-  }
+  int eso, ego, rso, rgo, cso, cgo;
+  chunk(kSwEY, yt - 2, eso, ego);
+  chunk(kSwRY, yt - 1, rso, rgo);
+  chunk(kSwCY, yt - 2, cso, cgo);
+  if (d.uni) cso = -1;
+  // ring slot of plane p (p >= -2; two's complement & keeps negatives in range)
   auto se_ = [](int p) { return p & (kSwNE - 1); };
+  auto sr_ = [](int p) { return p & (kSwNR - 1); };
   auto sc_ = [](int p) { return p & (kSwNC - 1); };
   auto load_e = [&](int p) {  // zero_src: the correction is zero (first sweep of a cycle on the finest level)
-    if (p < 0 || p >= d.nz) return;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-      if (ego[u] < 0) continue;
-      if (zero_src)
-        *(float4*)&sm.e[se_(p)][eso[u]] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      else
-        cp_async16(&sm.e[se_(p)][eso[u]], src + ego[u] + (long long)d.sz * p);
-    }
+    if (ego < 0 || p < 0 || p >= d.nz) return;
+    if (zero_src)
+      *(float4*)&sm.e[se_(p)][eso] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    else
+      cp_async16(&sm.e[se_(p)][eso], src + ego + (long long)d.sz * p);
+  };
+  auto load_r = [&](int p) {
+    if (rgo >= 0 && p >= 0 && p < d.nz) cp_async16(&sm.r[sr_(p)][rso], d.rhs + rgo + (long long)d.sz * p);
   };
   auto load_c = [&](int p) {
-    if (p < 0 || p >= d.nz) return;
-#pragma unroll
-    for (int u = 0; u < 2; u++)
-      if (cso[u] >= 0 && cgo[u] >= 0) cp_async4(&sm.c[sc_(p)][cso[u]], d.cd + cgo[u] + (long long)d.sz * p);
+    if (cso >= 0 && p >= 0 && p < d.nz) cp_async4(&sm.c[sc_(p)][cso], d.cd + cgo + (long long)d.sz * p);
   };
-  // this thread's update: 0 none, 1 odd quad of plane s, 2 even quad of plane
-  // s+2.  Quads 0..3 of a row cover the tile's 16 points of one colour; an
-  // even row's quad 4 covers its x-halo point (x = xt+32 in the even half or
-  // x = xt-1 in the odd half, whichever is even-coloured) and three more
-  // points that are computed but neither stored nor read.  Warps 0 and 1 take
-  // the odd quads of rows yt + w + 2i, warps 2 and 3 the even quads of rows
-  // yt - 1 + (w - 2) + 2i (i = lane >> 2, quad lane & 3): the rows of such a
-  // warp share their colour parity, so the half that holds a colour is the
-  // same across the warp, and a quarter warp's rows r and r + 2 start 16
-  // banks apart.  Warp 4 takes the even quads 0..3 of rows yt+15 and yt+16
-  // and the quads 4 of all 18 rows.
-  const int lane = tid & 31, wp = tid >> 5;
-  int role = 0, uy = 0, uq = lane & 3;
-  if (wp < 2) {
-    role = 1;
-    uy = yt + wp + 2 * (lane >> 2);
-  } else if (wp < 4) {
-    role = 2;
-    uy = yt - 1 + (wp - 2) + 2 * (lane >> 2);
-  } else if (lane < 8) {
-    role = 2;
-    uy = yt + 15 + (lane >> 2);
-  } else if (lane < 26) {
-    role = 2;
-    uq = 4;
-    uy = lane < 17 ? yt - 1 + 2 * (lane - 8) : yt + 2 * (lane - 17);
+  // this thread's points.  Main (first point): even point of row ym = yt-1+tid/16
+  // at x = xt + 2(tid%16) + ((xt + ym + p) & 1).  Second point: odd point of row
+  // yo = yt + tid/16 at x = xt + 2(tid%16) + ((xt + yo + p + 1) & 1), or for
+  // threads TY*16 .. TY*16+TY+1 the halo even point of row yh = yt-1+(tid-TY*16)
+  // at xt-1 or xt+TX, whichever has the even colour.
+  const int cm = tid & 15;
+  const int ym = yt - 1 + (tid >> 4);
+  const bool m_ok = ym >= 1 && ym <= d.ny - 2;
+  const int m_pb = (xt + ym) & 1, m_off = (ym - yt + 2) * kSwW + 4 + 2 * cm, m_g = xt + 2 * cm + d.sy * ym;
+  int o_kind = 0, o_y = 0, o_pb = 0, o_off = 0, o_g = 0;  // 1 odd point, 2 halo even point
+  if (tid < kSwTY * 16) {
+    o_y = yt + (tid >> 4);
+    o_kind = 1;
+    o_pb = (xt + o_y + 1) & 1;
+    o_off = (o_y - yt + 2) * kSwW + 4 + 2 * cm;
+    o_g = xt + 2 * cm + d.sy * o_y;
+  } else if (tid < kSwTY * 16 + kSwTY + 2) {
+    o_y = yt - 1 + (tid - kSwTY * 16);
+    o_kind = 2;
+    o_pb = (xt - 1 + o_y) & 1;  // 0: x = xt-1 is even-coloured in even planes
+    o_off = (o_y - yt + 2) * kSwW + 3;
+    o_g = xt - 1 + d.sy * o_y;
   }
-  const bool row_act = role != 0 && uy >= 1 && uy <= d.ny - 2;  // interior row
-  const bool own_row = uq < 4 && uy >= yt && uy < yt + kSwTY;
-  const int er = uy - (yt - 2);  // shared correction and code row of this thread's row
-  // shared element offset within a half-row of this thread's quad in half h
-  // (its first half-index is hx0 - 4 + offset)
-  auto qso = [&](int h) { return uq < 4 ? 4 + 4 * uq : (h ? 0 : 20); };
-  // the right-hand side of this thread's update of plane p (zero where it has none)
-  auto rhs_at = [&](int p) {
-    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const int h = role == 1 ? (1 + uy + p) & 1 : (uy + p) & 1, hi0 = hx0 - 4 + qso(h);
-    if (!row_act || p < 1 || p > d.nz - 2 || hi0 < 0 || hi0 >= hp) return v;
-    return __ldg(reinterpret_cast<const float4*>(d.rhs + (long long)d.sz * p + uy * d.sy + h * hp + hi0));
-  };
-  // the four points of a quad: half h, half-indices hi0 + k
-  auto quad = [&](int h, int p, bool own, const float4& rh) {
-    const int so = qso(h), hi0 = hx0 - 4 + so;
-    if (!row_act || p < 1 || p > d.nz - 2 || hi0 < 0 || hi0 >= hp) return;
-    float* E0 = sm.e[se_(p)] + er * kSwW;
-    const float* Em = sm.e[se_(p - 1)] + er * kSwW;
-    const float* Ep = sm.e[se_(p + 1)] + er * kSwW;
-    const float4 old = *(const float4*)&E0[h * kSwHW + so];
-    const float4 A = *(const float4*)&E0[(1 - h) * kSwHW + so];
-    const float B = E0[(1 - h) * kSwHW + (h ? so + 4 : so - 1)];
-    const float4 yp = *(const float4*)&E0[kSwW + h * kSwHW + so], ym = *(const float4*)&E0[-kSwW + h * kSwHW + so];
-    const float4 zp = *(const float4*)&Ep[h * kSwHW + so], zm = *(const float4*)&Em[h * kSwHW + so];
-    float4 xp, xm;
-    if (h) {  // odd x: x+1 is the next even point, x-1 the even point of the same index
-      xp = make_float4(A.y, A.z, A.w, B);
-      xm = A;
-    } else {  // even x: x+1 is the odd point of the same index, x-1 the previous one
-      xp = A;
-      xm = make_float4(B, A.x, A.y, A.z);
-    }
-    const int gb = p * d.sz + uy * d.sy + h * hp + hi0;  // split global index of the first point
-    float o[4] = {old.x, old.y, old.z, old.w};
-    const float vxp[4] = {xp.x, xp.y, xp.z, xp.w}, vxm[4] = {xm.x, xm.y, xm.z, xm.w};
-    const float vyp[4] = {yp.x, yp.y, yp.z, yp.w}, vym[4] = {ym.x, ym.y, ym.z, ym.w};
-    const float vzp[4] = {zp.x, zp.y, zp.z, zp.w}, vzm[4] = {zm.x, zm.y, zm.z, zm.w};
-    const float vr[4] = {rh.x, rh.y, rh.z, rh.w};
-    // point k (x = lo + 2k) is interior when k <= kmax and x >= 1
-    const int lo = 2 * hi0 + h, kmax = (d.nx - 2 - lo) >> 1;
-    const bool k0 = lo >= 1;
-    if (d.uni) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        if (k > kmax || (k == 0 && !k0)) continue;
-        const float ns = d.w6 * ((vxp[k] + vxm[k]) + (vyp[k] + vym[k]) + (vzp[k] + vzm[k]));
-        const float dg = 6.0f * d.w6;
-        const float gs = kSorMode ? (ns + vr[k]) / dg : __fdividef(ns + vr[k], dg);
-        const float dv = gs - o[k];
-        o[k] = o[k] + om * dv;
-        if (kSorMode && own) acc += (double)dv * (double)dv;
-      }
-    } else {
-      const uint8_t* C0 = sm.c[sc_(p)] + er * kSwCW;
-      const uint8_t* Cm = sm.c[sc_(p - 1)] + er * kSwCW;
-      const unsigned c0 = *(const unsigned*)&C0[h * kSwHW + so];
-      const unsigned cym = *(const unsigned*)&C0[-kSwCW + h * kSwHW + so];
-      const unsigned czm = *(const unsigned*)&Cm[h * kSwHW + so];
-      const unsigned w1 = *(const unsigned*)&C0[(1 - h) * kSwHW + so];
-      const unsigned cxm = h ? w1 : __funnelshift_r(*(const unsigned*)&C0[(1 - h) * kSwHW + so - 4], w1, 24);
-      // per point (one byte each): the eps_in bits of its six faces and its
-      // kappa flag, an index into tf, and whether a face crosses the surface
-      // (2-bit face code 2: the dielectric comes from the maps)
-      const unsigned pat =
-          (c0 & 0x55555555u) | (((cxm & 0x01010101u) | (cym & 0x04040404u) | (czm & 0x10101010u)) << 1);
-      const unsigned crs = (c0 & 0x2A2A2A2Au) | (cxm & 0x02020202u) | (cym & 0x08080808u) | (czm & 0x20202020u);
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        if (k > kmax || (k == 0 && !k0)) continue;
-        const unsigned pk = (pat >> (8 * k)) & 127u;
-        const float4 u = sm.tf[0][pk], v = sm.tf[1][pk];
-        float a = u.x, b = u.y, c = u.z, dd = u.w, f = v.x, g = v.y, sum = v.z;  // v.w: kappa-bar^2 term
-        if ((crs >> (8 * k)) & 0xFFu) {
-          const int gi = gb + k;
-          const unsigned q0 = c0 >> (8 * k), qx = cxm >> (8 * k), qy = cym >> (8 * k), qz = czm >> (8 * k);
-          const float *__restrict__ mx = maps[0], *__restrict__ my = maps[1], *__restrict__ mz = maps[2];
-          if (q0 & 2u) a = mx[gi];
-          if (qx & 2u) b = mx[ixm(gi, lo + 2 * k, hp)];
-          if (q0 & 8u) c = my[gi];
-          if (qy & 8u) dd = my[gi - d.sy];
-          if (q0 & 32u) f = mz[gi];
-          if (qz & 32u) g = mz[gi - d.sz];
-          sum = (a + b) + (c + dd) + (f + g);
-        }
-        const float ns = ((a * vxp[k] + b * vxm[k]) + (c * vyp[k] + dd * vym[k]) + (f * vzp[k] + g * vzm[k])) * d.ih;
-        const float dg = fmaf(sum, d.ih, v.w);
-        const float gs = kSorMode ? (ns + vr[k]) / dg : __fdividef(ns + vr[k], dg);
-        const float dv = gs - o[k];
-        o[k] = o[k] + om * dv;
-        if (kSorMode && own) acc += (double)dv * (double)dv;
-      }
-    }
-    *(float4*)&E0[h * kSwHW + so] = make_float4(o[0], o[1], o[2], o[3]);
-  };
-  auto even = [&](int p, const float4& rh) {
-    if (role == 2) quad((uy + p) & 1, p, own_row && p >= z0 && p < z1, rh);
-  };
-  auto odd = [&](int p, const float4& rh) {
-    if (role == 1) quad((1 + uy + p) & 1, p, own_row, rh);
-  };
-  // store of this thread: one float4 of a tile row half; warp w stores rows
-  // 4w .. 4w+3, a quarter warp the same half of rows r and r + 2
+  if (o_y < 1 || o_y > d.ny - 2) o_kind = 0;
+  // store of this thread: one aligned float4 of a tile row
   int sso = -1, sgo = 0;
-  if (tid < kSwTY * 2 * 4) {
-    const int pi = (tid >> 2) & 7, r = 4 * (tid >> 5) + ((pi & 1) << 1) + ((pi >> 1) & 1), hh = pi >> 2;
-    const int c = tid & 3, y = yt + r, hi = hx0 + 4 * c;
-    if (y < d.ny && hi + 4 <= hp) {
-      sso = (r + 2) * kSwW + hh * kSwHW + 4 + 4 * c;
-      sgo = y * d.sy + hh * hp + hi;
+  if (tid < kSwTY * (kSwTX / 4)) {
+    const int r = tid / (kSwTX / 4), c = tid % (kSwTX / 4), y = yt + r, x = xt + 4 * c;
+    if (y < d.ny && x < d.sy) {
+      sso = (r + 2) * kSwW + 4 * c + 4;
+      sgo = x + d.sy * y;
     }
   }
+  struct Planes {
+    float* E0;
+    const float *Em, *Ep, *R;
+    const uint8_t *C0, *Cm;
+    int gp;
+  };
+  auto planes = [&](int p) {
+    return Planes{sm.e[se_(p)], sm.e[se_(p - 1)], sm.e[se_(p + 1)], sm.r[sr_(p)],
+                  sm.c[sc_(p)], sm.c[sc_(p - 1)], d.sz * p};
+  };
+  auto update = [&](const Planes& P, int x, int off, int g, bool own) {
+    if (x < 1 || x > d.nx - 2) return;
+    const float dv = sw_update<kSorMode>(d, sm.tf, om, P.E0, P.Em, P.Ep, P.R, P.C0, P.Cm, off, g + P.gp);
+    if (kSorMode && own) acc += (double)dv * (double)dv;
+  };
+  const bool m_own = ym >= yt && ym < yt + kSwTY;  // first-point row inside the tile (not the y halo)
+  // even points of plane p: first point and x-halo point
+  auto even = [&](int p) {
+    if (p < 1 || p > d.nz - 2) return;
+    const Planes P = planes(p);
+    const int par = m_pb ^ (p & 1);
+    const bool own = p >= z0 && p < z1;
+    if (m_ok) update(P, xt + 2 * cm + par, m_off + par, m_g + par, own && m_own);
+    if (o_kind == 2) {
+      const int h = (o_pb ^ (p & 1)) ? kSwTX + 1 : 0;  // xt-1 or xt+TX
+      update(P, xt - 1 + h, o_off + h, o_g + h, false);
+    }
+  };
+  auto odd = [&](int p) {
+    if (o_kind != 1 || p < 1 || p > d.nz - 2) return;
+    const Planes P = planes(p);
+    const int par = o_pb ^ (p & 1);
+    update(P, xt + 2 * cm + par, o_off + par, o_g + par, true);
+  };
   auto store = [&](int p) {
     if (sso >= 0) *(float4*)(dst + sgo + (long long)d.sz * p) = *(const float4*)&sm.e[se_(p)][sso];
   };
@@ -682,44 +594,35 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
   // prologue: what the even points of planes z0-1 .. z0+1 and step z0 read,
   // then the planes of step z0+1
   for (int p = z0 - 2; p <= z0 + 3; p++) load_e(p);
+  for (int p = z0 - 1; p <= z0 + 2; p++) load_r(p);
   for (int p = z0 - 2; p <= z0 + 2; p++) load_c(p);
   cp_async_commit();
-  if (tid == 0) {
-    maps[0] = d.ex;
-    maps[1] = d.ey;
-    maps[2] = d.ez;
-  }
-  if (!d.uni && tid < 128) {  // face table (read after the barrier below)
+  if (!d.uni && tid < 64) {  // face table (read after the barrier below)
     const float a = (tid & 1) ? d.fin : d.fout, b = (tid & 2) ? d.fin : d.fout, c = (tid & 4) ? d.fin : d.fout,
                 dd = (tid & 8) ? d.fin : d.fout, f = (tid & 16) ? d.fin : d.fout, g = (tid & 32) ? d.fin : d.fout;
     sm.tf[0][tid] = make_float4(a, b, c, dd);
-    sm.tf[1][tid] = make_float4(f, g, (a + b) + (c + dd) + (f + g), (tid & 64) ? d.kb : 0.0f);
+    sm.tf[1][tid] = make_float4(f, g, (a + b) + (c + dd) + (f + g), 0.0f);
   }
   load_e(z0 + 4);
+  load_r(z0 + 3);
   load_c(z0 + 3);
   cp_async_commit();
-  float4 r0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), r1 = r0, r2 = r0;
-  if (role == 2) {
-    r0 = rhs_at(z0 - 1);
-    r1 = rhs_at(z0);
-    r2 = rhs_at(z0 + 1);
-  }
-  float4 rn = rhs_at(role == 1 ? z0 : z0 + 2);  // right-hand side of step z0's update
   cp_async_wait<1>();
   __syncthreads();
-  even(z0 - 1, r0);
-  even(z0, r1);
-  even(z0 + 1, r2);
+  even(z0 - 1);
+  even(z0);
+  even(z0 + 1);
   for (int s = z0; s < z1; s++) {
-    const float4 rc = rn;
-    cp_async_wait<1>();  // all groups but the newest: correction planes to s+3, codes to s+2
+    cp_async_wait<1>();  // all groups but the newest: correction planes to s+3, rhs / codes to s+2
     __syncthreads();
-    if (s + 5 <= z1 + 1) load_e(s + 5);  // the last step reads correction planes to z1+1, codes to z1
-    if (s + 4 <= z1) load_c(s + 4);
+    if (s + 5 <= z1 + 1) load_e(s + 5);  // the last step reads correction planes to z1+1, rhs / codes to z1
+    if (s + 4 <= z1) {
+      load_r(s + 4);
+      load_c(s + 4);
+    }
     cp_async_commit();
-    if (s + 1 < z1) rn = rhs_at(role == 1 ? s + 1 : s + 3);
-    if (s + 2 <= z1) even(s + 2, rc);
-    odd(s, rc);
+    if (s + 2 <= z1) even(s + 2);
+    odd(s);
     if (s > z0) store(s - 1);
   }
   __syncthreads();
@@ -730,6 +633,7 @@ __global__ void __launch_bounds__(kSwThreads, 4) k_sweep_t(WL w, const LvlD* __r
     if (threadIdx.x == 0) part[(long long)j * nparts + lb] = t;
   }
 }
+
 
 // SOR bookkeeping after a sweep and its update (pb_solver.rs:373-447): rms
 // of the sweep's updates from the sweep blocks' partial sums (fixed order),
@@ -745,7 +649,7 @@ __global__ void k_sor_norm(WL w, const JobD* __restrict__ J, JobState* __restric
   const JobD& d = J[j];
   const bool rel = d.rtol > 0.0;
   const int used = rel ? ((d.nx + 31) >> 5) * ((d.ny + 7) >> 3) * ((d.nz + 7) >> 3)
-                       : sweep_blocks(0, d.nx, d.ny, d.nz);
+                       : ((d.nx + kSwTX - 1) / kSwTX) * ((d.ny + kSwTY - 1) / kSwTY) * ((d.nz + kSwZC0 - 1) / kSwZC0);
   const double* src = rel ? rpart : part;
   double s = 0.0;
   for (int k = threadIdx.x; k < used; k += blockDim.x) s += src[(long long)j * nparts + k];
@@ -779,9 +683,9 @@ __global__ void __launch_bounds__(256) k_res32(WL w, const LvlD* __restrict__ L,
   for (int k = 0; k < 8; k++) {
     int z = z0 + k;
     if (z < 1 || z > d.nz - 2) continue;
-    int i = xo(x, d.hp) + d.sy * y + d.sz * z;
+    int i = x + d.sy * y + d.sz * z;
     float ns, dg;
-    st32(d, d.e2, x, i, ns, dg);
+    st32(d, d.e2, i, ns, dg);
     d.res[i] = d.rhs[i] + ns - dg * d.e2[i];
   }
 }
@@ -818,12 +722,12 @@ __global__ void __launch_bounds__(256) k_restrict32(WL w, const LvlD* __restrict
           int x = fx + dx;
           if (x < 0 || x >= f.nx) continue;
           float wt = wyz * (dx == 0 ? 2.0f : 1.0f);
-          sum += wt * res[xo(x, f.hp) + f.sy * y + f.sz * z];
+          sum += wt * res[x + f.sy * y + f.sz * z];
           ws += wt;
         }
       }
     }
-    int i = xo(cx, c.hp) + c.sy * cy + c.sz * cz;
+    int i = cx + c.sy * cy + c.sz * cz;
     c.rhs[i] = rsc * sum / ws;
     c.e[i] = 0.0f;
   }
@@ -853,14 +757,13 @@ __global__ void __launch_bounds__(256) k_prolong32(WL w, const LvlD* __restrict_
     if (fz >= f.nz || (skipb && (fz == 0 || fz == f.nz - 1))) continue;
     int z0 = min(fz >> 1, mz);
     float dz = (float)fz * 0.5f - (float)z0;
-    const float* b = ce + c.sy * y0 + c.sz * z0;
-    const int a0 = xo(x0, c.hp), a1 = xo(x0 + 1, c.hp);
-    float c00 = b[a0] * (1.0f - dx) + b[a1] * dx;
-    float c10 = b[c.sy + a0] * (1.0f - dx) + b[c.sy + a1] * dx;
-    float c01 = b[c.sz + a0] * (1.0f - dx) + b[c.sz + a1] * dx;
-    float c11 = b[c.sz + c.sy + a0] * (1.0f - dx) + b[c.sz + c.sy + a1] * dx;
+    const float* b = ce + x0 + c.sy * y0 + c.sz * z0;
+    float c00 = b[0] * (1.0f - dx) + b[1] * dx;
+    float c10 = b[c.sy] * (1.0f - dx) + b[c.sy + 1] * dx;
+    float c01 = b[c.sz] * (1.0f - dx) + b[c.sz + 1] * dx;
+    float c11 = b[c.sz + c.sy] * (1.0f - dx) + b[c.sz + c.sy + 1] * dx;
     float c0 = c00 * (1.0f - dy) + c10 * dy, c1 = c01 * (1.0f - dy) + c11 * dy;
-    f.e2[xo(fx, f.hp) + f.sy * fy + f.sz * fz] += c0 * (1.0f - dz) + c1 * dz;
+    f.e2[fx + f.sy * fy + f.sz * fz] += c0 * (1.0f - dz) + c1 * dz;
   }
 }
 
@@ -877,9 +780,9 @@ __global__ void k_coarse32(WL w, const LvlD* __restrict__ L, int lvl, const JobS
       for (int k = threadIdx.x; k < ni; k += blockDim.x) {
         int ix = 1 + k % nxi, iy = 1 + (k / nxi) % nyi, iz = 1 + k / (nxi * nyi);
         if (((ix + iy + iz + colour) & 1) != 0) continue;
-        int i = xo(ix, d.hp) + d.sy * iy + d.sz * iz;
+        int i = ix + d.sy * iy + d.sz * iz;
         float ns, dg;
-        st32(d, d.e, ix, i, ns, dg);
+        st32(d, d.e, i, ns, dg);
         float old = d.e[i];
         float gs = (ns + d.rhs[i]) / dg;
         d.e[i] = old + d.om * (gs - old);
@@ -992,7 +895,7 @@ __global__ void k_maps32(WL w, const JobD* __restrict__ J, const LvlD* __restric
   int n = d.nx * d.ny * d.nz;
   int i = lb * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const long long ci = xo(i % d.nx, d.px >> 1) + (long long)d.px * (i / d.nx);  // split FP32 index
+  const long long ci = i % d.nx + (long long)d.px * (i / d.nx);  // padded FP32 index
   ((float*)l0.ex)[ci] = (float)d.ex[i];
   ((float*)l0.ey)[ci] = (float)d.ey[i];
   ((float*)l0.ez)[ci] = (float)d.ez[i];
@@ -1015,7 +918,7 @@ __global__ void k_codes(WL w, const JobD* __restrict__ J, const LvlD* __restrict
   unsigned exc = 0, chg = 0;
   if (i < n) {
     const int x = i % d.nx, t = i / d.nx;
-    const long long ci = xo(x, d.px >> 1) + (long long)d.px * t;  // t = y + ny z
+    const long long ci = x + (long long)d.px * t;  // t = y + ny z
     unsigned c = 0;
     if (!d.uniform) {
       unsigned a = fcode(d.ex[i], d.din, d.dout), b = fcode(d.ey[i], d.din, d.dout), e = fcode(d.ez[i], d.din, d.dout);
@@ -1051,8 +954,8 @@ __global__ void k_inject32(WL w, const LvlD* __restrict__ L, int lvl) {
   int i = lb * blockDim.x + threadIdx.x;
   if (i >= cn) return;
   int cx = i % c.nx, cy = (i / c.nx) % c.ny, cz = i / (c.nx * c.ny);
-  int fi = xo(min(2 * cx, f.nx - 1), f.px >> 1) + f.px * (min(2 * cy, f.ny - 1) + f.ny * min(2 * cz, f.nz - 1));
-  int ci = xo(cx, c.px >> 1) + c.px * (cy + c.ny * cz);
+  int fi = min(2 * cx, f.nx - 1) + f.px * (min(2 * cy, f.ny - 1) + f.ny * min(2 * cz, f.nz - 1));
+  int ci = cx + c.px * (cy + c.ny * cz);
   ((float*)c.ex)[ci] = f.ex[fi];
   ((float*)c.ey)[ci] = f.ey[fi];
   ((float*)c.ez)[ci] = f.ez[fi];
@@ -1080,8 +983,7 @@ __device__ __forceinline__ float coarse_face(const LvlD& f, const float* __restr
       if (p[t1] < 0 || p[t1] >= n[t1] || p[t2] < 0 || p[t2] >= n[t2]) continue;
       int q[3] = {p[0], p[1], p[2]};
       q[axis] = min(p[axis] + 1, n[axis] - 1);
-      const float e0 = m[xo(p[0], f.px >> 1) + f.px * (p[1] + f.ny * p[2])],
-                  e1 = m[xo(q[0], f.px >> 1) + f.px * (q[1] + f.ny * q[2])];
+      const float e0 = m[p[0] + f.px * (p[1] + f.ny * p[2])], e1 = m[q[0] + f.px * (q[1] + f.ny * q[2])];
       if (!any) first = e0;
       any = true;
       same = same && e0 == first && e1 == first;
@@ -1103,8 +1005,8 @@ __global__ void k_coarsen32(WL w, const LvlD* __restrict__ L, int lvl) {
   if (i >= cn) return;
   int cx = i % c.nx, cy = (i / c.nx) % c.ny, cz = i / (c.nx * c.ny);
   int bx = min(2 * cx, f.nx - 1), by = min(2 * cy, f.ny - 1), bz = min(2 * cz, f.nz - 1);
-  int fi = xo(bx, f.px >> 1) + f.px * (by + f.ny * bz);
-  int ci = xo(cx, c.px >> 1) + c.px * (cy + c.ny * cz);
+  int fi = bx + f.px * (by + f.ny * bz);
+  int ci = cx + c.px * (cy + c.ny * cz);
   const float ex = coarse_face(f, f.ex, 0, bx, by, bz), ey = coarse_face(f, f.ey, 1, bx, by, bz),
               ez = coarse_face(f, f.ez, 2, bx, by, bz);
   ((float*)c.ex)[ci] = ex;
@@ -1177,8 +1079,7 @@ F64Lay f64_lay(const PbJob& J) {
   return f;
 }
 // FP32 and code arrays: rows padded to a multiple of 4 points (16 bytes of FP32)
-// split rows (see xo): half pitch = the even points of a row rounded up to 4
-int pitch(const PbGeom& g) { return 2 * (int)((((g.nx + 1) >> 1) + 3) & ~3); }
+int pitch(const PbGeom& g) { return (int)((g.nx + 3) & ~3); }
 size_t padded_n(const PbGeom& g) { return (size_t)pitch(g) * g.ny * g.nz; }
 
 long long nbricks(const PbGeom& g) { return cdiv(g.nx, 32) * cdiv(g.ny, 8) * cdiv(g.nz, 8); }
@@ -1316,7 +1217,6 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
   double* P64 = pool64_.as<double>();
   float* P32 = pool32_.as<float>();
   RSTG_CUDA(cudaMemsetAsync(P32, 0, b32, st));
-  RSTG_CUDA(cudaMemsetAsync(P8, 0, b8, st));  // split rows: padding codes are read (and ignored) with their row
 
   // ---- maps and boundary values (FP64, the reference's set-up) -------------
   // One grid's set-up is a chain of small launches with host waits (the
@@ -1483,7 +1383,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     s.om = 1.0;
     s.status = Y.nlev >= 0 ? kMg : kSor;
     max_res = std::max(max_res, nbricks(J.g));
-    max_sor = std::max(max_sor, (long long)sweep_blocks(0, J.g.nx, J.g.ny, J.g.nz));
+    max_sor = std::max(max_sor, cdiv(J.g.nx, kSwTX) * cdiv(J.g.ny, kSwTY) * cdiv(J.g.nz, kSwZC0));  // sweep blocks
     for (int l = 0; l <= std::max(Y.nlev, 0); l++) {
       const PbGeom& g = Y.lv[l];
       size_t m = padded_n(g);
@@ -1495,7 +1395,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       L.rhs = b + 2 * m;
       L.res = b + 3 * m;
       L.px = pitch(g);
-      L.zc = sweep_zc(l, g.nz);
+      L.zc = sweep_chunk(l);
       if (!J.uniform) {
         L.ex = b + 4 * m;
         L.ey = b + 5 * m;
@@ -1745,14 +1645,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
     s_sor = lists.add_slot();
     s_snorm = lists.add_slot();
     any_mg = any_sor = false;
-    // grids with dielectric maps first: their blocks take longest, and blocks
-    // start in list order, so the short constant-coefficient blocks fill the
-    // tail of each launch
-    std::vector<int> order;
-    for (int pass = 0; pass < 2; pass++)
-      for (int j = 0; j < nj; j++)
-        if (jobs[j].uniform == (pass == 1)) order.push_back(j);
-    for (int j : order) {
+    for (int j = 0; j < nj; j++) {
       const Lay& Y = lay[j];
       const PbGeom& g = jobs[j].g;
       if (hs[j].status == kMg) {
@@ -1760,7 +1653,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
         maxlev = std::max(maxlev, Y.nlev);
         for (int l = 0; l < Y.nlev; l++) {
           const PbGeom& a = Y.lv[l];
-          lists.add(ls[l].rb, j, sweep_blocks(l, a.nx, a.ny, a.nz));
+          lists.add(ls[l].rb, j, cdiv(a.nx, kSwTX) * cdiv(a.ny, kSwTY) * cdiv(a.nz, sweep_chunk(l)));
           lists.add(ls[l].res, j, nbricks(a));
           lists.add(ls[l].restr, j, nbricks(Y.lv[l + 1]));
           lists.add(ls[l].prol, j, nbricks(a));
@@ -1771,7 +1664,7 @@ void PbBatchEngine::solve(std::vector<PbJob>& jobs, const rstg_pb_params& p, con
       } else if (hs[j].status == kSor) {
         any_sor = true;
         lists.add(s_sres, j, nbricks(g));
-        lists.add(s_sor, j, sweep_blocks(0, g.nx, g.ny, g.nz));
+        lists.add(s_sor, j, cdiv(g.nx, kSwTX) * cdiv(g.ny, kSwTY) * cdiv(g.nz, kSwZC0));
         lists.add(s_snorm, j, 1);
       }
     }
