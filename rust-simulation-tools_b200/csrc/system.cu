@@ -49,11 +49,15 @@ namespace rstg {
 static constexpr float kSasaBand = 2e-4f;
 static constexpr float kNbGuard2 = 3.5f * 3.5f;
 
-// shared memory of a k_sasa block of `warps` warps
+// distance classes of k_sasa's neighbour order, per part (own, other)
+static constexpr int kSasaBins = 8;
+// A^-1: class width 0.8 A of centre-to-centre distance (the last class is open)
+static constexpr float kSasaBinScale = 1.25f;
+
+// shared memory of a k_sasa block of `warps` warps: per warp the ordered
+// neighbours, each entry's class and slot, its atom, and the class counts
 static size_t sasa_smem(int cap, int warps) {
-  size_t cap2 = 32;
-  while ((int)cap2 < cap) cap2 <<= 1;
-  return (size_t)warps * (cap * sizeof(float4) + cap2 * (sizeof(float) + sizeof(int)));
+  return (size_t)warps * (cap * (sizeof(float4) + 2 * sizeof(int)) + 2 * kSasaBins * sizeof(int));
 }
 
 struct GbConstF {
@@ -748,70 +752,59 @@ __global__ void k_sasa(int nC, int nR, int cap, const int* __restrict__ nbr, con
                        const double* __restrict__ sph64, double* __restrict__ sasa, int* __restrict__ diag) {
   extern __shared__ float4 snb[];  // [warps][cap] (rel x, rel y, rel z, thr)
   int nw = blockDim.x >> 5;
-  int cap2 = 32;
-  while (cap2 < cap) cap2 <<= 1;
-  float* skey = (float*)(snb + nw * cap);  // [warps][cap2] sort keys
-  int* sval = (int*)(skey + nw * cap2);    // [warps][cap2] list positions, then atom indices
+  int* stag = (int*)(snb + nw * cap);  // [warps][cap] class << 16 | slot within the class
+  int* sval = stag + nw * cap;         // [warps][cap] atom of each ordered entry
+  int* shist = sval + nw * cap;        // [warps][2 * kSasaBins] class counts, then class offsets
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int i = blockIdx.x * nw + w, f = blockIdx.y;
   if (i >= nC) return;
   float4* nb = snb + w * cap;
-  float* key = skey + w * cap2;
-  int* val = sval + w * cap2;
+  int* tag = stag + w * cap;
+  int* val = sval + w * cap;
+  int* hist = shist + w * 2 * kSasaBins;
   long long o = (long long)f * nC + i;
   int cnt = min(nbrcnt[o], cap);
-  int c2 = 32;  // sort length: this atom's neighbours rounded up to a power of two
-  while (c2 < cnt) c2 <<= 1;
   const int* L = nbr + o * cap;
   const float4* X = xyz32 + (long long)f * nC;
   const double* X64 = xyz64 + (long long)f * nC * 3;
   float4 xi = X[i];
   bool in_r = i < nR;
-  // Order the neighbours: own part first, then the other part, each nearest
-  // first.  Near neighbours bury the largest caps, so buried points (nearly
-  // all of them) exit after a test or two.  Order does not change which
-  // points are accessible.
-  int n_own = 0;
-  for (int k = lane; k < c2; k += 32) {
-    if (k < cnt) {
-      int j = L[k];
-      float4 xj = X[j];
-      float rx = xj.x - xi.x, ry = xj.y - xi.y, rz = xj.z - xi.z;
-      bool own = (j < nR) == in_r;
-      key[k] = fmaf(rx, rx, fmaf(ry, ry, rz * rz)) + (own ? 0.f : 1.0e6f);
-      val[k] = j;
-    } else {
-      key[k] = 3.0e38f;
-      val[k] = -1;
-    }
-  }
-  for (int k0 = 0; k0 < cnt; k0 += 32) {
-    int k = k0 + lane;
-    bool own = k < cnt && ((L[k] < nR) == in_r);
-    n_own += __popc(__ballot_sync(0xffffffffu, own));
+  // Order the neighbours: own part first, then the other part, each by
+  // distance class (0.8 A classes, nearest first; any order inside a class),
+  // by a counting sort.  Near neighbours bury the largest caps, so buried
+  // points (nearly all of them) exit after a test or two.  Order does not
+  // change which points are accessible.
+  if (lane < 2 * kSasaBins) hist[lane] = 0;
+  __syncwarp();
+  for (int k = lane; k < cnt; k += 32) {
+    const int j = L[k];
+    const float4 xj = X[j];
+    const float rx = xj.x - xi.x, ry = xj.y - xi.y, rz = xj.z - xi.z;
+    const float d = sqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
+    const int cls = min((int)(d * kSasaBinScale), kSasaBins - 1) + (((j < nR) == in_r) ? 0 : kSasaBins);
+    tag[k] = (cls << 16) | atomicAdd(&hist[cls], 1);
   }
   __syncwarp();
-  for (int size = 2; size <= c2; size <<= 1)  // bitonic sort of (key, val)
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int t = lane; t < c2 / 2; t += 32) {
-        int a = 2 * t - (t & (stride - 1)), b = a + stride;
-        bool up = (a & size) == 0;
-        float ka = key[a], kb = key[b];
-        if ((ka > kb) == up) {
-          key[a] = kb;
-          key[b] = ka;
-          int v = val[a];
-          val[a] = val[b];
-          val[b] = v;
-        }
-      }
-      __syncwarp();
+  int n_own = 0;
+  if (lane < 2 * kSasaBins) {  // exclusive prefix sum of the class counts
+    const int c = hist[lane];
+    int incl = c;
+#pragma unroll
+    for (int sh = 1; sh < 2 * kSasaBins; sh <<= 1) {
+      const int t = __shfl_up_sync(0xffffu, incl, sh);
+      if (lane >= sh) incl += t;
     }
+    hist[lane] = incl - c;
+    if (lane == kSasaBins - 1) n_own = incl;
+  }
+  n_own = __shfl_sync(0xffffffffu, n_own, kSasaBins - 1);
+  __syncwarp();
   for (int k = lane; k < cnt; k += 32) {
-    int j = val[k];
-    float4 xj = X[j];
-    float ro = (float)(rad64[j] + probe);
-    nb[k] = make_float4(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, ro * ro);
+    const int t = tag[k], j = L[k], q = hist[t >> 16] + (t & 0xffff);
+    const float4 xj = X[j];
+    const float ro = (float)(rad64[j] + probe);
+    val[q] = j;
+    nb[q] = make_float4(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, ro * ro);
   }
   __syncwarp();
   double er = rad64[i] + probe;
