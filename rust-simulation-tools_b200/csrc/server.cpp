@@ -8,7 +8,14 @@
 // oldest on the highest priority): the device hands freed SMs to the oldest
 // request's blocks first, so a large request is not stretched by the small
 // ones that fill the gaps, and at every chunk boundary the ranks are taken
-// again.  Per-request latency (submit -> results ready) is recorded.
+// again.  Stream priorities cannot displace the blocks of a persistent kernel
+// that is already resident, so the device work in flight is capped as well:
+// a GB chunk of about a full chunk's pair evaluations fills the device, and
+// chunks run beside it only while the work in flight stays under 1.5 full
+// chunks; a request whose chunk does not fit holds back every younger one
+// except tiny chunks (a tenth of a full one at most), so large requests run
+// in arrival order at full speed while small ones overlap.  Per-request
+// latency (submit -> results ready) is recorded.
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -27,6 +34,10 @@ namespace rstg {
 
 using Clock = std::chrono::steady_clock;
 
+// complex pair evaluations of a full GB chunk, the cap on those in flight,
+// and the largest chunk that may pass an older request waiting for room
+constexpr double kChunkWork = 2.5e9, kWorkCap = 1.5 * kChunkWork, kTinyWork = 0.1 * kChunkWork;
+
 struct Request {
   int64_t id = 0;
   System* sys = nullptr;
@@ -35,6 +46,7 @@ struct Request {
   std::vector<rstg_frame_energy> out;
   int64_t bytes = 0;
   int64_t chunk = 1;     // frames per chunk
+  double work_per_frame = 0.0;  // complex pair evaluations per frame (GB engine; 0: not capped)
   int64_t next = 0;      // first frame not yet dispatched
   int64_t done = 0;      // frames finished
   bool in_flight = false;
@@ -65,6 +77,7 @@ struct Server {
   int64_t use_clock = 0;
   int64_t resident_total = 0, peak_bytes = 0, next_id = 1, frames_done = 0;
   int running = 0;
+  double inflight_work = 0.0;  // pair evaluations of the GB chunks in flight
   bool stop = false;
   int64_t device_bytes = 0;  // a request whose buffers exceed the device is refused at submit
   std::vector<double> latencies_ms;
@@ -143,7 +156,7 @@ struct Server {
     else if (sys->solv.method == 1)
       c = 16;
     else
-      c = (int64_t)(2.5e9 / std::max(1.0, (double)sys->nC * (double)sys->nC));
+      c = (int64_t)(kChunkWork / std::max(1.0, (double)sys->nC * (double)sys->nC));
     return std::max<int64_t>(1, std::min(c, std::max<int64_t>(F, 1)));
   }
 
@@ -178,15 +191,28 @@ struct Server {
     }
   }
 
+  double chunk_work(const Request& r) const {
+    return r.work_per_frame * (double)std::min(r.chunk, r.n_frames - r.next);
+  }
+
   // Next chunk to run: of the oldest request that has frames left, no chunk
-  // in flight and an idle system; a request's first chunk also needs its
-  // buffers to fit the budget after evicting idle systems (a request larger
-  // than the whole budget is admitted alone when nothing else runs, so it
-  // cannot starve).
+  // in flight and an idle system, whose chunk keeps the work in flight under
+  // kWorkCap (anything runs on an idle device); once an older request waits
+  // for room, only tiny chunks may pass it.  A request's first chunk also
+  // needs its buffers to fit the budget after evicting idle systems (a
+  // request larger than the whole budget is admitted alone when nothing else
+  // runs, so it cannot starve).
   std::shared_ptr<Request> pick() {
+    bool held = false;  // an older request waits for the work in flight to drain
     for (auto& r : queue) {
       if (r->in_flight || r->next >= r->n_frames || r->state == Request::CANCELLED) continue;
       if (busy.count(r->sys)) continue;
+      const double w = chunk_work(*r);
+      if (running > 0 && inflight_work + w > kWorkCap) {
+        held = true;
+        continue;
+      }
+      if (held && w > kTinyWork) continue;
       if (!r->admitted) {
         int64_t need = growth(*r);
         evict_for(need, r->sys);
@@ -213,6 +239,7 @@ struct Server {
     for (;;) {
       std::shared_ptr<Request> r;
       int64_t f0 = 0, B = 0;
+      double work = 0.0;
       cudaStream_t st = nullptr;
       {
         std::unique_lock<std::mutex> lk(mu);
@@ -223,6 +250,8 @@ struct Server {
         busy[r->sys] = 1;
         last_use[r->sys] = ++use_clock;
         running++;
+        work = chunk_work(*r);
+        inflight_work += work;
         f0 = r->next;
         B = std::min(r->chunk, r->n_frames - f0);
         r->next += B;
@@ -258,6 +287,7 @@ struct Server {
         std::lock_guard<std::mutex> lk(mu);
         busy.erase(r->sys);
         running--;
+        inflight_work -= work;
         r->in_flight = false;
         r->done += B;
         if (r->state == Request::CANCELLED) {
@@ -288,6 +318,8 @@ struct Server {
     r->frames.assign(frames, frames + (size_t)F * sys->n_top * 3);
     r->out.resize(F);
     r->chunk = chunk_for(sys, F);
+    if (sys->opts.mode == RSTG_MODE_FUSED && sys->solv.method != 1)
+      r->work_per_frame = (double)sys->nC * (double)sys->nC;
     r->bytes = sys->footprint(std::min<int64_t>(r->chunk, sys->batch > 0 ? sys->batch : r->chunk));
     if (r->bytes > device_bytes)
       throw Error(RSTG_ERR_NOMEM, "request needs " + std::to_string(r->bytes) + " bytes of device memory; the device has " +

@@ -147,14 +147,24 @@ __device__ __forceinline__ double self64(double q, double R, const GbConstF& k) 
 // reference expression equals (1/r) sum_k k/(2k+1) x^(2k+1), x = s/r.  The
 // series has no cancellation; truncated after k = 6 it is exact to 1e-8
 // relative for x <= 1/4.
-__device__ __forceinline__ float hct_far(float x, float rinv) {
-  float x2 = x * x;
+// In terms of u = 1/r^2 and the column's s^2, s^3: x^2 = s^2 u and
+// x^3 / r = s^3 u^2.
+__device__ __forceinline__ float hct_far(float s2, float s3, float u) {
+  const float x2 = s2 * u;
   float p = fmaf(x2, 6.0f / 13.0f, 5.0f / 11.0f);
   p = fmaf(x2, p, 4.0f / 9.0f);
   p = fmaf(x2, p, 3.0f / 7.0f);
   p = fmaf(x2, p, 2.0f / 5.0f);
   p = fmaf(x2, p, 1.0f / 3.0f);
-  return x * x2 * rinv * p;
+  return (s3 * u) * (u * p);
+}
+
+// reciprocal with the special-function unit's approximation (relative error
+// about 2^-23, the order of the FP32 rounding of the series it feeds)
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
 
 // One block per 128 rows (atoms i) of a frame, all columns j in 128-wide
@@ -174,7 +184,7 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
   constexpr int kCols = kTile / TPR, kWords = kCols / 32;
   static_assert(kCols % 32 == 0, "columns per thread in whole words");
   __shared__ float4 sx[kTile];
-  __shared__ float2 sp[kTile];
+  __shared__ float4 sp[kTile];  // column atom: s, s^2, s^3, SASA reach
   __shared__ double sh[32];
   __shared__ int scnt[kTile];
   __shared__ double2 spsi[TPR > 1 ? kTile * (TPR - 1) : 1];
@@ -198,7 +208,7 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
       if (jl < nC) {
         sx[threadIdx.x] = X[jl];
         float4 pj = P32[jl];
-        sp[threadIdx.x] = make_float2(pj.z, pj.w);
+        sp[threadIdx.x] = make_float4(pj.z, pj.z * pj.z, pj.z * pj.z * pj.z, pj.w);
       }
     }
     __syncthreads();
@@ -218,17 +228,19 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
           float4 xj = sx[jj];
           float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
           float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          float2 s = sp[jj];
-          float ee = ext_i + s.y;
+          float4 s = sp[jj];
+          float ee = ext_i + s.w;
           if (j != i && r2 <= fmaf(ee * ee, 1.00001f, 1e-4f)) {
             int c = TPR > 1 ? atomicAdd(&scnt[row], 1) : scnt[row]++;
             if (c < cap) my[c] = j;
           }
           if (j == i || r2 > k.fcut2) continue;
-          float rinv = rsqrtf(r2), r = r2 * rinv, sj = s.x;
           bool own = (j < nR) == in_r;
-          if (r2 > 0.f && 16.f * sj * sj <= r2 && rho_i <= r - sj) {
-            float t = hct_far(sj * rinv, rinv);
+          // far field: s <= r / 4 and rho_i + s <= r (a pair with rho_i + s < 0
+          // that fails the squared test takes the exact FP64 path)
+          const float rs = rho_i + s.x;
+          if (r2 > 0.f && 16.f * s.y <= r2 && rs * rs <= r2) {
+            float t = hct_far(s.y, s.z, rcp_approx(r2));
             if (own)
               po += t;
             else
