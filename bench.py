@@ -630,6 +630,21 @@ def main():
             extras["plain_gpu"] = {"value": pv, "unit": "frames/s", "sample_frames": args.plain_frames,
                                    "form": "FP64, one subsystem per launch sequence, per frame, decomposition"}
             extras["speedup_vs_plain_gpu"] = value / world / pv
+            # the middle form: the same FP32-pair / FP64-reduction kernels with
+            # one frame per launch sequence, so the gain of batching stands
+            # apart from that of the precision split
+            sysm = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, gb_params=gb, sa_params=sa,
+                                     batch_frames=1, ctx=ctx)
+            nm = 4 * args.plain_frames
+            sysm.run(fr[:1], decompose=True)
+            t = time.perf_counter()
+            sysm.run(fr[:nm], decompose=True)
+            mv = nm / (time.perf_counter() - t)
+            extras["mixed_unbatched"] = {"value": mv, "unit": "frames/s", "sample_frames": nm,
+                                         "form": "FP32 pairs with FP64 reductions, binding-fused kernels, "
+                                                 "one frame per launch sequence (batch of 1)",
+                                         "speedup_vs_plain_gpu": mv / pv,
+                                         "batched_speedup_over_it": value / world / mv}
         if rank == 0 and world == 1 and args.ref_frames > 0:
             extras["cpu_baseline"] = cpu_baseline(s, fr, args.ref_frames, out_np, d_dec.cpu().numpy())
         if rank == 0 and world == 1 and args.serve_requests > 0:

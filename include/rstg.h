@@ -382,6 +382,19 @@ rstg_status rstg_system_profile(rstg_system* s, const float* d_frames, int64_t n
  * nominal maximum SM clock in MHz. */
 rstg_status rstg_calibrate(int device, double* out4);
 
+/* Periodic reimaging of the system's complex, reimage_complex
+ * (crates/mmpbsa/src/binding.rs:234-308): bonded components unwrapped along
+ * a breadth-first walk of the bond graph, then each component after the
+ * first moved to the minimum image of the first one's geometric centre.
+ * frames: F frames in topology order [F][n_atoms][3] Angstrom, boxes [F][3]
+ * edge lengths, both host memory; out (may equal frames) receives the frames
+ * with the complex atoms reimaged and the other atoms as given.
+ * on_device 1: one block per frame on the GPU; 0: on the host.  Both forms
+ * use the reference's FP64 operations in its order and give the same bits.
+ * The trajectory workflow below reimages boxed frames on the device. */
+rstg_status rstg_system_reimage(rstg_system* s, const double* frames, const double* boxes, int64_t n_frames,
+                                int32_t on_device, double* out);
+
 /* compute_binding_energy over a trajectory file, crates/mmpbsa/src/binding.rs:461-744.
  * format: "dcd" or "mdcrd".  frames_out may be NULL; stats9 = mean_delta_mm,
  * mean_delta_polar, mean_delta_sa, mean_delta_total, std_delta_total,

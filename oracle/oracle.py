@@ -411,3 +411,71 @@ def read_dcd_nm(path: str) -> np.ndarray:
     out = np.zeros((nf, na.value, 3))
     lib().orc_read_dcd(path.encode(), _d(out), out.size, C.byref(na), err, 512)
     return out
+
+
+def reimage_complex(coords_A, bonds, box):
+    """Restatement of reimage_complex (crates/mmpbsa/src/binding.rs:234-308)
+    in plain Python floats, for small cases: unwrap every bonded component
+    along a breadth-first walk (starts in atom order, neighbours in bond
+    order; an atom found from `current` moves by one box edge where it sits
+    more than half an edge from it), then move every component after the
+    first by one box edge where its geometric centre (binding.rs:311-322, sum
+    in visit order divided by the count) sits more than half an edge from the
+    first one's.  coords_A: (n, 3); bonds: (a, b) pairs; box: 3 edges.
+    Returns a new (n, 3) float64 array."""
+    x = [[float(v) for v in row] for row in np.asarray(coords_A, dtype=np.float64)]
+    box = [float(b) for b in box]
+    n = len(x)
+    if n == 0:
+        return np.zeros((0, 3))
+    adj = [[] for _ in range(n)]
+    for a, b in bonds:
+        if a < n and b < n:
+            adj[a].append(b)
+            adj[b].append(a)
+    seen = [False] * n
+    comps = []
+    for s in range(n):
+        if seen[s]:
+            continue
+        comp, queue, head = [], [s], 0
+        seen[s] = True
+        while head < len(queue):
+            cur = queue[head]
+            head += 1
+            comp.append(cur)
+            for nb in adj[cur]:
+                if seen[nb]:
+                    continue
+                seen[nb] = True
+                for d in range(3):
+                    diff = x[nb][d] - x[cur][d]
+                    if diff > box[d] * 0.5:
+                        x[nb][d] -= box[d]
+                    elif diff < -box[d] * 0.5:
+                        x[nb][d] += box[d]
+                queue.append(nb)
+        comps.append(comp)
+
+    def centre(c):
+        m = [0.0, 0.0, 0.0]
+        for a in c:
+            for d in range(3):
+                m[d] += x[a][d]
+        return [v / float(len(c)) for v in m]
+
+    if len(comps) > 1:
+        ref = centre(comps[0])
+        for c in comps[1:]:
+            cc = centre(c)
+            sh = [0.0, 0.0, 0.0]
+            for d in range(3):
+                diff = cc[d] - ref[d]
+                if diff > box[d] * 0.5:
+                    sh[d] = -box[d]
+                elif diff < -box[d] * 0.5:
+                    sh[d] = box[d]
+            for a in c:
+                for d in range(3):
+                    x[a][d] += sh[d]
+    return np.array(x, dtype=np.float64)

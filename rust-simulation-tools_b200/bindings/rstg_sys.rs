@@ -319,6 +319,8 @@ extern "C" {
     pub fn rstg_system_profile(s: *mut rstg_system, d_frames: *const f32, n_frames: i64, n: *mut i32,
                                names: *mut c_char, ms: *mut f64, flops: *mut f64, bytes: *mut f64) -> rstg_status;
     pub fn rstg_calibrate(device: c_int, out4: *mut f64) -> rstg_status;
+    pub fn rstg_system_reimage(s: *mut rstg_system, frames: *const f64, boxes: *const f64, n_frames: i64,
+                               on_device: i32, out: *mut f64) -> rstg_status;
     pub fn rstg_binding_trajectory(ctx: *mut rstg_ctx, t: *const rstg_topology, path: *const c_char,
                                    format: *const c_char, has_box: i32, receptor_residues: *const i64, n_rec: i64,
                                    ligand_residues: *const i64, n_lig: i64, solv: *const rstg_solvation,

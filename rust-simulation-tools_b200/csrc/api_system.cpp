@@ -7,6 +7,7 @@
 
 #include "internal.hpp"
 #include "system.hpp"
+#include "reimage.hpp"
 #include "trajectory.hpp"
 
 namespace rstg {
@@ -32,68 +33,6 @@ static std::vector<int64_t> vec(const int64_t* p, int64_t n) {
   if (n < 0) throw Error(RSTG_ERR_INVALID, "negative length");
   if (n > 0 && !p) throw Error(RSTG_ERR_INVALID, "null array with non-zero length");
   return std::vector<int64_t>(p, p + n);
-}
-
-// reimage_complex, binding.rs:234-308: unwrap bonded components by BFS and
-// shift every component to the minimum image of the first one's centre.
-static void reimage(double* x, int64_t n, const Topology& t, const std::array<double, 3>& box) {
-  if (n == 0) return;
-  std::vector<std::vector<int64_t>> adj(n);
-  for (size_t b = 0; b < t.bond_i.size(); b++) {
-    int64_t a = t.bond_i[b], c = t.bond_j[b];
-    if (a < n && c < n) {
-      adj[a].push_back(c);
-      adj[c].push_back(a);
-    }
-  }
-  std::vector<uint8_t> vis(n, 0);
-  std::vector<std::vector<int64_t>> comps;
-  for (int64_t s = 0; s < n; s++) {
-    if (vis[s]) continue;
-    std::vector<int64_t> comp;
-    std::deque<int64_t> q{s};
-    vis[s] = 1;
-    while (!q.empty()) {
-      int64_t cur = q.front();
-      q.pop_front();
-      comp.push_back(cur);
-      for (int64_t nb : adj[cur]) {
-        if (vis[nb]) continue;
-        vis[nb] = 1;
-        for (int d = 0; d < 3; d++) {
-          double diff = x[3 * nb + d] - x[3 * cur + d];
-          if (diff > box[d] * 0.5)
-            x[3 * nb + d] -= box[d];
-          else if (diff < -box[d] * 0.5)
-            x[3 * nb + d] += box[d];
-        }
-        q.push_back(nb);
-      }
-    }
-    comps.push_back(std::move(comp));
-  }
-  if (comps.size() <= 1) return;
-  auto centre = [&](const std::vector<int64_t>& c) {
-    std::array<double, 3> m{0, 0, 0};
-    for (int64_t a : c)
-      for (int d = 0; d < 3; d++) m[d] += x[3 * a + d];
-    for (int d = 0; d < 3; d++) m[d] /= (double)c.size();
-    return m;
-  };
-  auto ref = centre(comps[0]);
-  for (size_t k = 1; k < comps.size(); k++) {
-    auto cc = centre(comps[k]);
-    double sh[3] = {0, 0, 0};
-    for (int d = 0; d < 3; d++) {
-      double diff = cc[d] - ref[d];
-      if (diff > box[d] * 0.5)
-        sh[d] = -box[d];
-      else if (diff < -box[d] * 0.5)
-        sh[d] = box[d];
-    }
-    for (int64_t a : comps[k])
-      for (int d = 0; d < 3; d++) x[3 * a + d] += sh[d];
-  }
 }
 
 }  // namespace rstg
@@ -270,6 +209,43 @@ rstg_status rstg_system_profile(rstg_system* s, const float* d_frames, int64_t F
   });
 }
 
+rstg_status rstg_system_reimage(rstg_system* s, const double* frames, const double* boxes, int64_t F,
+                                int32_t on_device, double* out) {
+  return guard([&] {
+    if (!s || (F > 0 && (!frames || !boxes || !out))) throw Error(RSTG_ERR_INVALID, "system, frames, boxes and out are required");
+    if (F < 0) throw Error(RSTG_ERR_INVALID, "F must be >= 0");
+    const int64_t n = s->n_top;
+    const Split& sp = s->split;
+    if (F == 0) return;
+    if (out != frames) memcpy(out, frames, (size_t)F * n * 24);
+    if (!on_device) {
+      std::vector<double> cx(sp.complex.n_atoms * 3);
+      for (int64_t f = 0; f < F; f++) {
+        double* x = out + (size_t)f * n * 3;
+        for (int64_t a = 0; a < sp.complex.n_atoms; a++) {
+          const int64_t ta = sp.complex_atoms.empty() ? a : sp.complex_atoms[a];
+          for (int d = 0; d < 3; d++) cx[3 * a + d] = x[3 * ta + d];
+        }
+        reimage_host(cx.data(), sp.complex.n_atoms, sp.complex, {boxes[3 * f], boxes[3 * f + 1], boxes[3 * f + 2]});
+        for (int64_t a = 0; a < sp.complex.n_atoms; a++) {
+          const int64_t ta = sp.complex_atoms.empty() ? a : sp.complex_atoms[a];
+          for (int d = 0; d < 3; d++) x[3 * ta + d] = cx[3 * a + d];
+        }
+      }
+      return;
+    }
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    Ctx* c = s->ctx;
+    c->bind();
+    DevBuf d_fr((size_t)F * n * 24, c->stream), d_bx((size_t)F * 24, c->stream);
+    RSTG_CUDA(cudaMemcpyAsync(d_fr.p, out, (size_t)F * n * 24, cudaMemcpyHostToDevice, c->stream));
+    RSTG_CUDA(cudaMemcpyAsync(d_bx.p, boxes, (size_t)F * 24, cudaMemcpyHostToDevice, c->stream));
+    reimage_device(c, c->stream, sp, n, d_fr.as<double>(), d_bx.as<double>(), F);
+    RSTG_CUDA(cudaMemcpyAsync(out, d_fr.p, (size_t)F * n * 24, cudaMemcpyDeviceToHost, c->stream));
+    RSTG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
 rstg_status rstg_binding_trajectory(rstg_ctx* c, const rstg_topology* t, const char* path, const char* format,
                                     int32_t has_box, const int64_t* rr, int64_t nr, const int64_t* lr, int64_t nl,
                                     const rstg_solvation* solv, const rstg_sa_params* sa, int64_t stride,
@@ -309,20 +285,21 @@ rstg_status rstg_binding_trajectory(rstg_ctx* c, const rstg_topology* t, const c
     std::unique_ptr<rstg_system, void (*)(rstg_system*)> hold(sys, rstg_system_destroy);
     std::vector<double> frames(sel.size() * n * 3);
     const Split& sp = sys->split;
-    for (size_t k = 0; k < sel.size(); k++) {
-      double* dst = &frames[k * n * 3];
-      memcpy(dst, &all[(size_t)sel[k] * n * 3], n * 24);
-      if (!boxes.empty()) {
-        std::vector<double> cx(sp.complex.n_atoms * 3);
-        for (int64_t a = 0; a < sp.complex.n_atoms; a++) {
-          int64_t ta = sp.complex_atoms.empty() ? a : sp.complex_atoms[a];
-          for (int d = 0; d < 3; d++) cx[3 * a + d] = dst[3 * ta + d];
-        }
-        reimage(cx.data(), sp.complex.n_atoms, sp.complex, boxes[sel[k]]);
-        for (int64_t a = 0; a < sp.complex.n_atoms; a++) {
-          int64_t ta = sp.complex_atoms.empty() ? a : sp.complex_atoms[a];
-          for (int d = 0; d < 3; d++) dst[3 * ta + d] = cx[3 * a + d];
-        }
+    for (size_t k = 0; k < sel.size(); k++) memcpy(&frames[k * n * 3], &all[(size_t)sel[k] * n * 3], n * 24);
+    if (!boxes.empty()) {  // reimaged on the device, in chunks of at most 512 MB of frames
+      std::vector<double> bx(sel.size() * 3);
+      for (size_t k = 0; k < sel.size(); k++)
+        for (int d = 0; d < 3; d++) bx[3 * k + d] = boxes[sel[k]][d];
+      c->bind();
+      const int64_t per = std::max<int64_t>(1, (int64_t)(512ll << 20) / std::max<int64_t>(n * 24, 1));
+      for (int64_t f0 = 0; f0 < (int64_t)sel.size(); f0 += per) {
+        const int64_t F = std::min<int64_t>(per, (int64_t)sel.size() - f0);
+        DevBuf d_fr((size_t)F * n * 24, c->stream), d_bx((size_t)F * 24, c->stream);
+        RSTG_CUDA(cudaMemcpyAsync(d_fr.p, &frames[f0 * n * 3], (size_t)F * n * 24, cudaMemcpyHostToDevice, c->stream));
+        RSTG_CUDA(cudaMemcpyAsync(d_bx.p, &bx[f0 * 3], (size_t)F * 24, cudaMemcpyHostToDevice, c->stream));
+        reimage_device(c, c->stream, sp, n, d_fr.as<double>(), d_bx.as<double>(), F);
+        RSTG_CUDA(cudaMemcpyAsync(&frames[f0 * n * 3], d_fr.p, (size_t)F * n * 24, cudaMemcpyDeviceToHost, c->stream));
+        RSTG_CUDA(cudaStreamSynchronize(c->stream));
       }
     }
     std::vector<rstg_frame_energy> res(sel.size());

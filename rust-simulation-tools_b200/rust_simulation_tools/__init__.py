@@ -756,6 +756,22 @@ class BindingSystem:
                                     dec.ctypes.data_as(C.POINTER(N.ResidueEnergy)) if decompose else None))
         return (out, dec) if decompose else out
 
+    def reimage(self, frames_A, boxes, on_device: bool = True) -> np.ndarray:
+        """Periodic reimaging of the complex atoms of each frame
+        (reimage_complex, binding.rs:234-308): frames (F, n_atoms, 3)
+        float64 Angstrom in topology order, boxes (F, 3) edge lengths.
+        Returns the reimaged frames (the other atoms as given)."""
+        fr = np.ascontiguousarray(frames_A, dtype=np.float64)
+        bx = np.ascontiguousarray(boxes, dtype=np.float64)
+        if fr.ndim != 3 or fr.shape[1:] != (self.n_atoms, 3):
+            raise ValueError(f"frames must have shape (F, {self.n_atoms}, 3)")
+        if bx.shape != (fr.shape[0], 3):
+            raise ValueError(f"boxes must have shape ({fr.shape[0]}, 3)")
+        out = np.empty_like(fr)
+        check(N.lib.rstg_system_reimage(self._h, fr.ctypes.data_as(N.dp), bx.ctypes.data_as(N.dp), fr.shape[0],
+                                        int(bool(on_device)), out.ctypes.data_as(N.dp)))
+        return out
+
     def run_device(self, d_frames: int, n_frames: int, d_out: int, d_decomp: int = 0) -> None:
         """Device pointers (e.g. torch ``data_ptr()``): frames float32
         [F][n_atoms][3], out float64 [F][13], decomp float64 [F][n_res][4]."""

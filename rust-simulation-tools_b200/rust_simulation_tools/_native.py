@@ -151,6 +151,7 @@ _sig("rstg_system_set_pb_convergence", C.c_int, vp, dbl)
 _sig("rstg_system_pb_profile", C.c_int, vp, dp)
 _sig("rstg_system_profile", C.c_int, vp, vp, i64, P(i32), C.c_char_p, dp, dp, dp)
 _sig("rstg_calibrate", C.c_int, C.c_int, dp)
+_sig("rstg_system_reimage", C.c_int, vp, dp, dp, i64, i32, dp)
 _sig("rstg_binding_trajectory", C.c_int, vp, vp, cs, cs, i32, ip, i64, ip, i64, P(Solvation), P(SaParams), i64,
      i64, i64, i32, P(FrameEnergy), i64, ip, dp, dp)
 _sig("rstg_server_opts_default", None, P(ServerOpts))

@@ -62,3 +62,37 @@ def test_wrapped_boxed_trajectory_reimages_to_intact(rst, tmp_path):
                                    mode="plain", **kw)
     ec = np.array([f.as_array() for f in c.frames])
     assert np.abs(ec[:, 10] - ea[:, 10]).max() > 1e-3
+
+
+def test_device_reimage_matches_host_and_oracle(rst, tmp_path):
+    """The device form (one block per frame, the walk's levels in order) and
+    the host form of reimage_complex give the bits of the restatement
+    (oracle.reimage_complex) on wrapped frames with per-frame cells: a
+    150-atom bonded chain (walk depth 149), several components, the
+    ligand a component of its own."""
+    import oracle as O
+    from rust_simulation_tools import synthetic as S
+
+    s = S.make_system(300, 24, seed=71)
+    ptr = list(s.residue_pointers) + [s.n_atoms]
+    bonds = [(a, a + 1) for r in range(len(ptr) - 1) for a in range(ptr[r], ptr[r + 1] - 1)]
+    nres_rec = len(s.receptor_residues)
+    bonds += [(ptr[r + 1] - 1, ptr[r + 1]) for r in range(nres_rec // 2)]  # chain the first half of the receptor
+    prm = str(tmp_path / "chain.prmtop")
+    S.write_prmtop(s, prm, bonds=bonds)
+    top = rst.read_prmtop(prm)
+    bs = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues,
+                           gb_params=rst.GbParams(model=rst.GbModel.ObcII), sa_params=rst.SaParams(n_sphere_points=120))
+    rng = np.random.default_rng(72)
+    fr = S.make_frames(s, 5, seed=73).astype(np.float64) + rng.uniform(-30, 30, size=(5, 1, 3))
+    boxes = rng.uniform(38.0, 70.0, size=(5, 3))
+    wrapped = fr - boxes[:, None, :] * np.floor(fr / boxes[:, None, :])
+    dev = bs.reimage(wrapped, boxes, on_device=True)
+    host = bs.reimage(wrapped, boxes, on_device=False)
+    assert np.array_equal(dev, host)
+    for f in range(5):
+        want = O.reimage_complex(wrapped[f], bonds, boxes[f])
+        assert np.array_equal(host[f], want), f
+    assert not np.array_equal(dev, wrapped)  # the frames were torn and have been mended
+    twice = bs.reimage(dev, boxes, on_device=True)  # a mended frame stays as it is
+    assert np.array_equal(twice, dev)

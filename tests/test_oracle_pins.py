@@ -136,3 +136,20 @@ def test_prmtop_dcd_roundtrip(oracle, small_system):
     nm = oracle.read_dcd_nm(dcd)
     assert nm.shape == fr.shape
     np.testing.assert_allclose(nm * 10.0, fr, atol=1e-5)
+
+
+def test_reimage_known_answer():
+    """reimage_complex (binding.rs:234-308) by hand: a three-atom chain torn
+    across the x faces of a 10 A cell is unwrapped along its bonds from atom
+    0, and a lone atom whose centre sits more than half a cell from the
+    chain's centre moves by one cell edge towards it."""
+    import oracle as O
+
+    x = [[9.5, 5.0, 5.0], [0.25, 5.0, 5.0], [1.0, 5.0, 5.0], [0.5, 5.0, 9.75]]
+    out = O.reimage_complex(x, [(0, 1), (1, 2)], [10.0, 10.0, 10.0])
+    # 0.25 - 9.5 < -5: +10; 1.0 - 10.25 < -5: +10; centre (9.5 + 10.25 + 11) / 3
+    # = 10.25 vs 0.5 on x: +10; z: 9.75 - 5 < 5 stays
+    want = [[9.5, 5.0, 5.0], [10.25, 5.0, 5.0], [11.0, 5.0, 5.0], [10.5, 5.0, 9.75]]
+    assert out.tolist() == want
+    # a component found later keeps its own start; no bonds, one atom: unchanged
+    assert O.reimage_complex([[3.0, 4.0, 5.0]], [], [10.0, 10.0, 10.0]).tolist() == [[3.0, 4.0, 5.0]]
