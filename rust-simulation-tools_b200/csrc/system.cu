@@ -63,6 +63,7 @@ static size_t sasa_smem(int cap, int warps) {
 struct GbConstF {
   double kappa, inv_ein, inv_eout, diel_ns, cut2;
   float fk, fie, fio, fdns, fcut2;
+  float tile_far2;  // A^2: k_psi tile pairs farther apart hold no SASA neighbours and only far-field pairs
   int no_salt, model;
   double rgbmax;
 };
@@ -167,13 +168,46 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return y;
 }
 
+// Bounding box of the points x (valid lanes) held by a block's warps: warp
+// minima / maxima into red[warp][6]; the caller's next barrier publishes them
+// and box_of() combines them.
+__device__ __forceinline__ void box_part(float4 x, bool valid, float (*red)[6]) {
+  float v[6] = {valid ? x.x : 3e38f, valid ? x.y : 3e38f, valid ? x.z : 3e38f,
+                valid ? x.x : -3e38f, valid ? x.y : -3e38f, valid ? x.z : -3e38f};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      v[d] = fminf(v[d], __shfl_xor_sync(0xffffffffu, v[d], o));
+      v[3 + d] = fmaxf(v[3 + d], __shfl_xor_sync(0xffffffffu, v[3 + d], o));
+    }
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int d = 0; d < 6; d++) red[threadIdx.x >> 5][d] = v[d];
+}
+__device__ __forceinline__ void box_of(const float (*red)[6], int warps, float (&b)[6]) {
+  for (int d = 0; d < 3; d++) {
+    b[d] = 3e38f;
+    b[3 + d] = -3e38f;
+  }
+  for (int w = 0; w < warps; w++)
+    for (int d = 0; d < 3; d++) {
+      b[d] = fminf(b[d], red[w][d]);
+      b[3 + d] = fmaxf(b[3 + d], red[w][3 + d]);
+    }
+}
+
 // One block per 128 rows (atoms i) of a frame, all columns j in 128-wide
 // shared-memory tiles.  TPR threads share a row, each taking a fixed share
 // of every tile's columns (TPR and the register cap MINB are picked per
 // system by the tuner); the row's shares are added in a fixed order, and its
 // SASA neighbour list is filled through a shared-memory counter (entry order
 // does not matter: k_sasa orders the list itself and a point's burial does
-// not depend on the order of its tests).
+// not depend on the order of its tests).  Slots are ordered along a Morton
+// curve, so a tile is a compact blob: when the bounding boxes of the row and
+// column tiles are farther apart than k.tile_far2, no pair between them is a
+// SASA neighbour or outside the HCT far field, and the block runs the tile
+// without those tests (the same sums the tests would give).
 template <int TPR, int MINB>
 __global__ void __launch_bounds__(kTile * TPR, MINB)
     k_psi(int nC, int nR, const float4* __restrict__ xyz32, const double* __restrict__ xyz64,
@@ -188,6 +222,8 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
   __shared__ double sh[32];
   __shared__ int scnt[kTile];
   __shared__ double2 spsi[TPR > 1 ? kTile * (TPR - 1) : 1];
+  __shared__ float sbox[2][kTile * TPR / 32][6];  // warp parts of the row tile's and a column tile's boxes
+  __shared__ float srow[6];                       // the row tile's box
   const int row = threadIdx.x % kTile, cpart = threadIdx.x / kTile, cb = cpart * kCols;
   int f = blockIdx.y, i = blockIdx.x * kTile + row;
   bool valid = i < nC;
@@ -202,22 +238,55 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
   int near64 = 0;
   if (cpart == 0) scnt[row] = 0;
   int* my = nbr + ((long long)f * nC + (valid ? i : 0)) * cap;
+  constexpr int kWarpsB = kTile * TPR / 32;
+  box_part(xi, valid, sbox[0]);
+  __syncthreads();
+  if (threadIdx.x < 6) {  // published by the first column tile's barrier
+    float v = sbox[0][0][threadIdx.x];
+    for (int w = 1; w < kWarpsB; w++)
+      v = threadIdx.x < 3 ? fminf(v, sbox[0][w][threadIdx.x]) : fmaxf(v, sbox[0][w][threadIdx.x]);
+    srow[threadIdx.x] = v;
+  }
   for (int j0 = 0; j0 < nC; j0 += kTile) {
-    if (threadIdx.x < kTile) {
+    float4 xs = make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool staged = threadIdx.x < kTile && j0 + (int)threadIdx.x < nC;
+    if (staged) {
       int jl = j0 + threadIdx.x;
-      if (jl < nC) {
-        sx[threadIdx.x] = X[jl];
-        float4 pj = P32[jl];
-        sp[threadIdx.x] = make_float4(pj.z, pj.z * pj.z, pj.z * pj.z * pj.z, pj.w);
-      }
+      xs = X[jl];
+      sx[threadIdx.x] = xs;
+      float4 pj = P32[jl];
+      sp[threadIdx.x] = make_float4(pj.z, pj.z * pj.z, pj.z * pj.z * pj.z, pj.w);
     }
+    box_part(xs, staged, sbox[1]);
     __syncthreads();
+    float cbx[6];
+    box_of(sbox[1], kWarpsB, cbx);
+    float gap2 = 0.f;  // squared distance between the two boxes
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const float g = fmaxf(0.f, fmaxf(cbx[d] - srow[3 + d], srow[d] - cbx[3 + d]));
+      gap2 = fmaf(g, g, gap2);
+    }
+    const bool far_tile = j0 != blockIdx.x * kTile && gap2 > k.tile_far2;
     int m = min(cb + kCols, nC - j0);
     float po = 0.f, pc = 0.f;
     unsigned nearm[kWords];  // tile columns that take the FP64 near path
 #pragma unroll
     for (int w = 0; w < kWords; w++) nearm[w] = 0u;
-    if (valid) {
+    if (valid && far_tile) {  // every pair far field, no neighbours, j != i
+      for (int jj = cb; jj < m; jj++) {
+        const float4 xj = sx[jj];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (r2 > k.fcut2) continue;
+        const float4 s = sp[jj];
+        const float t = hct_far(s.y, s.z, rcp_approx(r2));
+        if (((j0 + jj) < nR) == in_r)
+          po += t;
+        else
+          pc += t;
+      }
+    } else if (valid) {
 #pragma unroll
       for (int w = 0; w < kWords; w++) {  // one mask word per step: the word stays in a register
         const int lo = cb + 32 * w, hi = min(lo + 32, m);
@@ -1412,6 +1481,18 @@ void System::prepare_fused(const double* x0) {
   k.fio = (float)k.inv_eout;
   k.fdns = (float)k.diel_ns;
   k.fcut2 = (float)std::min(k.cut2, 3.0e38);
+  {
+    // the largest SASA reach and HCT far-field bound over all atoms, with a
+    // margin for the FP32 rounding of the box distance and of r^2
+    double ext = 0.0, sm = 0.0, rm = 0.0;
+    for (int64_t a = 0; a < nC; a++) {
+      ext = std::max(ext, (double)P[a].w);
+      sm = std::max(sm, std::fabs((double)P[a].z));
+      rm = std::max(rm, std::fabs((double)P[a].y));
+    }
+    const double far2 = std::max({4.0 * ext * ext * 1.00001 + 1e-4, 16.0 * sm * sm, (rm + sm) * (rm + sm)});
+    k.tile_far2 = (float)(far2 * 1.001 + 0.01);
+  }
   k.model = g.model;
   k.rgbmax = g.rgbmax;
   // neighbour capacity from the first frame (x1.5 + 32 margin; re-sized on overflow)
