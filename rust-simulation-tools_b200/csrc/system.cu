@@ -527,7 +527,9 @@ __device__ __forceinline__ void pair_word(int lo, int hi, int first, int j0, int
     if (is14 || (!excl && r2 < kNbGuard2)) {
       dfr |= 1u << b;
     } else if (!excl) {
-      const float2 ab = slj[P.ti * nt + st[jj]];
+      // the column's type selects the table row (one for the warp) and the
+      // lanes' row types spread over it: few shared-memory bank conflicts
+      const float2 ab = slj[st[jj] * nt + P.ti];
       const float rinv = rsqrtf(r2), ir2 = rinv * rinv, ir6 = ir2 * ir2 * ir2;
       a[P.in_r ? 4 : 5] += fmaf(ab.x * ir6, ir6, fmaf(-ab.y, ir6, qq * rinv));
     }
@@ -572,7 +574,7 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
             double scnb, double* __restrict__ part, int* __restrict__ diag) {
   constexpr int kCols = kTile / TPR, kWords = kCols / 32, kWarps = kTile * TPR / 32;
   static_assert(kCols % 32 == 0, "columns per thread in whole words");
-  extern __shared__ float2 slj[];  // nt*nt (A, B)
+  extern __shared__ float2 slj[];  // nt*nt (A, B), [column type][row type]
   __shared__ float4 sx[kTile];
   __shared__ float4 sR[kTile];
   __shared__ float sdR[kTile];
@@ -693,7 +695,7 @@ __global__ void __launch_bounds__(256, MINB)
               const double2* __restrict__ lj64, const unsigned* __restrict__ masks, GbConstF k, double scee,
               double scnb, double* __restrict__ part, int* __restrict__ diag) {
   constexpr int kCols = kTile / H, kWords = kCols / 32, kSub = 4 * H;
-  extern __shared__ float2 slj[];  // nt*nt (A, B)
+  extern __shared__ float2 slj[];  // nt*nt (A, B), [column type][row type]
   for (int t = threadIdx.x; t < nt * nt; t += blockDim.x) slj[t] = lj32[t];
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -1357,7 +1359,7 @@ void System::prepare_fused(const double* x0) {
       int64_t idx = C.nb_index[C.n_types * a + b];
       if (idx >= 1) {
         l64[a * nt + b] = make_double2(C.lj_a[idx - 1], C.lj_b[idx - 1]);
-        l32[a * nt + b] = make_float2((float)C.lj_a[idx - 1], (float)C.lj_b[idx - 1]);
+        l32[b * nt + a] = make_float2((float)C.lj_a[idx - 1], (float)C.lj_b[idx - 1]);  // column type major
       }
     }
   up(F.lj32, l32.data(), l32.size() * sizeof(float2));
