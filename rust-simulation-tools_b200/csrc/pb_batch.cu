@@ -287,19 +287,25 @@ __global__ void __launch_bounds__(256, 4) k_upres64(WL w, const JobD* __restrict
   int x, y, z0;
   brick_col(lb, nx, ny, x, y, z0);
   double acc = 0.0;
-  if (x < nx && y < ny) {
+  if (x < nx && y < ny && z0 < nz) {
     const bool inxy = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
     int i = x + sy * y + sz * z0, ci = x + cy * y + cz * z0;  // FP64 and padded FP32 / code indices
+    // phi + e along the column in registers: the planes below, at and above
+    // the current point (the z neighbours are not loaded again)
+    double vm = (inxy && z0 >= 1) ? p[i - sz] + (double)e0[ci - cz] : 0.0;
+    double vc = p[i] + (double)e0[ci];
 #pragma unroll 1
     for (int k = 0; k < 8; k++, i += sz, ci += cz) {
       const int z = z0 + k;
       if (z >= nz) break;
-      const double v = p[i] + (double)e0[ci];
+      const double v = vc;
+      const double vzp = z + 1 < nz ? p[i + sz] + (double)e0[ci + cz] : 0.0, vzm = vm;
+      vm = vc;
+      vc = vzp;
       q[i] = v;
       if (!inxy || z < 1 || z > nz - 2) continue;
       const double vxp = p[i + 1] + (double)e0[ci + 1], vxm = p[i - 1] + (double)e0[ci - 1],
-                   vyp = p[i + sy] + (double)e0[ci + cy], vym = p[i - sy] + (double)e0[ci - cy],
-                   vzp = p[i + sz] + (double)e0[ci + cz], vzm = p[i - sz] + (double)e0[ci - cz];
+                   vyp = p[i + sy] + (double)e0[ci + cy], vym = p[i - sy] + (double)e0[ci - cy];
       const unsigned c0 = cd[ci];
       double ns, dg;
       if (uni) {
