@@ -169,9 +169,8 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return y;
 }
 
-// Bounding box of the points x (valid lanes) held by a block's warps: warp
-// minima / maxima into red[warp][6]; the caller's next barrier publishes them
-// and box_of() combines them.
+// Bounding box of the points x (valid lanes) of each warp of a block: warp
+// minima / maxima into red[warp][6], published by the caller's next barrier.
 __device__ __forceinline__ void box_part(float4 x, bool valid, float (*red)[6]) {
   float v[6] = {valid ? x.x : 3e38f, valid ? x.y : 3e38f, valid ? x.z : 3e38f,
                 valid ? x.x : -3e38f, valid ? x.y : -3e38f, valid ? x.z : -3e38f};
@@ -186,17 +185,6 @@ __device__ __forceinline__ void box_part(float4 x, bool valid, float (*red)[6]) 
 #pragma unroll
     for (int d = 0; d < 6; d++) red[threadIdx.x >> 5][d] = v[d];
 }
-__device__ __forceinline__ void box_of(const float (*red)[6], int warps, float (&b)[6]) {
-  for (int d = 0; d < 3; d++) {
-    b[d] = 3e38f;
-    b[3 + d] = -3e38f;
-  }
-  for (int w = 0; w < warps; w++)
-    for (int d = 0; d < 3; d++) {
-      b[d] = fminf(b[d], red[w][d]);
-      b[3 + d] = fmaxf(b[3 + d], red[w][3 + d]);
-    }
-}
 
 // One block per 128 rows (atoms i) of a frame, all columns j in 128-wide
 // shared-memory tiles.  TPR threads share a row, each taking a fixed share
@@ -205,10 +193,11 @@ __device__ __forceinline__ void box_of(const float (*red)[6], int warps, float (
 // SASA neighbour list is filled through a shared-memory counter (entry order
 // does not matter: k_sasa orders the list itself and a point's burial does
 // not depend on the order of its tests).  Slots are ordered along a Morton
-// curve, so a tile is a compact blob: when the bounding boxes of the row and
-// column tiles are farther apart than k.tile_far2, no pair between them is a
-// SASA neighbour or outside the HCT far field, and the block runs the tile
-// without those tests (the same sums the tests would give).
+// curve, so 32 consecutive slots are a compact blob: when the bounding boxes
+// of a warp's 32 rows and of a 32-column chunk are farther apart than
+// k.tile_far2, no pair between them is a SASA neighbour or outside the HCT
+// far field, and the warp runs the chunk without those tests (the same sums
+// the tests would give).
 template <int TPR, int MINB>
 __global__ void __launch_bounds__(kTile * TPR, MINB)
     k_psi(int nC, int nR, const float4* __restrict__ xyz32, const double* __restrict__ xyz64,
@@ -224,7 +213,6 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
   __shared__ int scnt[kTile];
   __shared__ double2 spsi[TPR > 1 ? kTile * (TPR - 1) : 1];
   __shared__ float sbox[2][kTile * TPR / 32][6];  // warp parts of the row tile's and a column tile's boxes
-  __shared__ float srow[6];                       // the row tile's box
   const int row = threadIdx.x % kTile, cpart = threadIdx.x / kTile, cb = cpart * kCols;
   int f = blockIdx.y, i = blockIdx.x * kTile + row;
   bool valid = i < nC;
@@ -239,15 +227,8 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
   int near64 = 0;
   if (cpart == 0) scnt[row] = 0;
   int* my = nbr + ((long long)f * nC + (valid ? i : 0)) * cap;
-  constexpr int kWarpsB = kTile * TPR / 32;
-  box_part(xi, valid, sbox[0]);
-  __syncthreads();
-  if (threadIdx.x < 6) {  // published by the first column tile's barrier
-    float v = sbox[0][0][threadIdx.x];
-    for (int w = 1; w < kWarpsB; w++)
-      v = threadIdx.x < 3 ? fminf(v, sbox[0][w][threadIdx.x]) : fmaxf(v, sbox[0][w][threadIdx.x]);
-    srow[threadIdx.x] = v;
-  }
+  box_part(xi, valid, sbox[0]);  // this warp's 32 rows; published by the first column tile's barrier
+  const float* rbox = sbox[0][threadIdx.x >> 5];
   for (int j0 = 0; j0 < nC; j0 += kTile) {
     float4 xs = make_float4(0.f, 0.f, 0.f, 0.f);
     const bool staged = threadIdx.x < kTile && j0 + (int)threadIdx.x < nC;
@@ -258,40 +239,44 @@ __global__ void __launch_bounds__(kTile * TPR, MINB)
       float4 pj = P32[jl];
       sp[threadIdx.x] = make_float4(pj.z, pj.z * pj.z, pj.z * pj.z * pj.z, pj.w);
     }
-    box_part(xs, staged, sbox[1]);
+    box_part(xs, staged, sbox[1]);  // the column tile's 32-column chunks (one per staging warp)
     __syncthreads();
-    float cbx[6];
-    box_of(sbox[1], kWarpsB, cbx);
-    float gap2 = 0.f;  // squared distance between the two boxes
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const float g = fmaxf(0.f, fmaxf(cbx[d] - srow[3 + d], srow[d] - cbx[3 + d]));
-      gap2 = fmaf(g, g, gap2);
-    }
-    const bool far_tile = j0 != blockIdx.x * kTile && gap2 > k.tile_far2;
     int m = min(cb + kCols, nC - j0);
     float po = 0.f, pc = 0.f;
     unsigned nearm[kWords];  // tile columns that take the FP64 near path
 #pragma unroll
     for (int w = 0; w < kWords; w++) nearm[w] = 0u;
-    if (valid && far_tile) {  // every pair far field, no neighbours, j != i
-      for (int jj = cb; jj < m; jj++) {
-        const float4 xj = sx[jj];
-        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        if (r2 > k.fcut2) continue;
-        const float4 s = sp[jj];
-        const float t = hct_far(s.y, s.z, rcp_approx(r2));
-        if (((j0 + jj) < nR) == in_r)
-          po += t;
-        else
-          pc += t;
-      }
-    } else if (valid) {
+    if (valid) {
 #pragma unroll
       for (int w = 0; w < kWords; w++) {  // one mask word per step: the word stays in a register
         const int lo = cb + 32 * w, hi = min(lo + 32, m);
         unsigned nw = 0u;
+        // this warp's rows against the chunk's columns: boxes farther apart than
+        // k.tile_far2 (so no atom in common) hold only far-field pairs and no
+        // SASA neighbours (a decision uniform over the warp)
+        const float* cbox = sbox[1][lo >> 5];
+        float gap2 = 0.f;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const float g = fmaxf(0.f, fmaxf(cbox[d] - rbox[3 + d], rbox[d] - cbox[3 + d]));
+          gap2 = fmaf(g, g, gap2);
+        }
+        if (lo < hi && gap2 > k.tile_far2) {
+#pragma unroll 2
+          for (int jj = lo; jj < hi; jj++) {
+            const float4 xj = sx[jj];
+            const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (r2 > k.fcut2) continue;
+            const float4 s = sp[jj];
+            const float t = hct_far(s.y, s.z, rcp_approx(r2));
+            if (((j0 + jj) < nR) == in_r)
+              po += t;
+            else
+              pc += t;
+          }
+          continue;
+        }
 #pragma unroll 2
         for (int jj = lo; jj < hi; jj++) {
           int j = j0 + jj;
@@ -1659,7 +1644,10 @@ void System::tune(const void* frames, bool f64, bool host_in, int64_t F) {
   }
   cudaStream_t st = stream();
   const int64_t B = std::min(F, batch);
-  int64_t TB = std::min<int64_t>(batch, std::max<int64_t>(std::min<int64_t>(B, 64), (2048 + fp->ntiles - 1) / fp->ntiles));
+  // the candidates run on the batch the first call will launch (at least 2,048
+  // pair-kernel work items): a shape's wave count and tail at that size decide,
+  // which a smaller trial batch misjudges
+  int64_t TB = std::min<int64_t>(batch, std::max<int64_t>(B, (2048 + fp->ntiles - 1) / fp->ntiles));
   TB = std::max<int64_t>(TB, 1);
   ensure_buffers(TB);
   const size_t fb = (size_t)n_top * 3 * (f64 ? 8 : 4);
