@@ -64,7 +64,7 @@ struct GbConstF {
   double kappa, inv_ein, inv_eout, diel_ns, cut2;
   float fk, fie, fio, fdns, fcut2;
   float fkl;        // -fk log2(e): E = 2^(fkl f)
-  float tile_far2;  // A^2: k_psi tile pairs farther apart hold no SASA neighbours and only far-field pairs
+  float tile_far2;  // A^2: k_psi row and column groups whose boxes are farther apart hold no SASA neighbours and only far-field pairs
   int no_salt, model;
   double rgbmax;
 };
