@@ -390,7 +390,7 @@ struct PsiVariant {
   int tpr, minb;
   PsiFn fn;
 };
-static const PsiVariant kPsiVariants[] = {{1, 8, k_psi<1, 8>}, {2, 4, k_psi<2, 4>}, {1, 1, k_psi<1, 1>}};
+static const PsiVariant kPsiVariants[] = {{1, 8, k_psi<1, 8>}, {2, 4, k_psi<2, 4>}, {1, 6, k_psi<1, 6>}};
 constexpr int kNumPsiVariants = (int)(sizeof(kPsiVariants) / sizeof(kPsiVariants[0]));
 
 // ---------------------------------------------------------------------------
@@ -805,7 +805,7 @@ struct PairsVariant {
 };
 static const PairsVariant kPairsVariants[] = {{0, 2, 4, 1, k_pairs<2, 4>}, {0, 1, 6, 1, k_pairs<1, 6>},
                                               {1, 1, 4, 4, k_pairs_w<1, 4>}, {1, 2, 4, 8, k_pairs_w<2, 4>},
-                                              {1, 1, 3, 4, k_pairs_w<1, 3>}, {1, 2, 3, 8, k_pairs_w<2, 3>}};
+                                              {1, 1, 3, 4, k_pairs_w<1, 3>}, {0, 2, 3, 1, k_pairs<2, 3>}};
 constexpr int kMaxPairsSub = 8;
 constexpr int kNumPairsVariants = (int)(sizeof(kPairsVariants) / sizeof(kPairsVariants[0]));
 static const int kSasaWarpChoices[] = {2, 4, 8};
