@@ -803,9 +803,9 @@ struct PairsVariant {
   int warp, tpr, minb, sub;
   PairsFn fn;
 };
-static const PairsVariant kPairsVariants[] = {{0, 2, 4, 1, k_pairs<2, 4>}, {0, 1, 6, 1, k_pairs<1, 6>},
-                                              {1, 1, 4, 4, k_pairs_w<1, 4>}, {1, 2, 4, 8, k_pairs_w<2, 4>},
-                                              {1, 1, 3, 4, k_pairs_w<1, 3>}, {0, 2, 3, 1, k_pairs<2, 3>}};
+static const PairsVariant kPairsVariants[] = {{0, 2, 3, 1, k_pairs<2, 3>}, {0, 2, 4, 1, k_pairs<2, 4>},
+                                              {0, 1, 6, 1, k_pairs<1, 6>}, {1, 1, 4, 4, k_pairs_w<1, 4>},
+                                              {1, 2, 4, 8, k_pairs_w<2, 4>}, {1, 1, 3, 4, k_pairs_w<1, 3>}};
 constexpr int kMaxPairsSub = 8;
 constexpr int kNumPairsVariants = (int)(sizeof(kPairsVariants) / sizeof(kPairsVariants[0]));
 static const int kSasaWarpChoices[] = {2, 4, 8};
