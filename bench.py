@@ -477,6 +477,9 @@ def main():
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the serving leg (--serve-requests over --serve-systems) and print it")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e/plain/cpu/serving legs")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="fixed launch shapes (the tuner's usual picks on B200) instead of timing candidates on "
+                         "the first run: for profiling, where the profiler distorts the candidates' timings")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -527,7 +530,8 @@ def main():
     S.write_prmtop(s, os.path.join(d, "w.prmtop"))
     top = rst.read_prmtop(os.path.join(d, "w.prmtop"))
     gb, sa = rst.GbParams(**GB), rst.SaParams(n_sphere_points=NPTS)
-    sysf = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, gb_params=gb, sa_params=sa, ctx=ctx)
+    sysf = rst.BindingSystem(top, s.receptor_residues, s.ligand_residues, gb_params=gb, sa_params=sa, ctx=ctx,
+                             autotune=not args.no_autotune)
     F, nres = fr.shape[0], sysf.n_residues
     d_fr = torch.from_numpy(fr).cuda()
     d_out = torch.empty((F, 13), dtype=torch.float64, device="cuda")

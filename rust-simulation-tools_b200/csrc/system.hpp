@@ -38,7 +38,7 @@ struct System {
   int pairs_variant = 0;  // index into the k_pairs shape table (system.cu)
   int psi_variant = 0;    // index into the k_psi shape table
   int pairs_per_sm[8] = {};  // resident k_pairs blocks per SM of each shape (persistent grid), 0 until queried
-  int sasa_warps = 4;     // warps (atoms) per k_sasa block
+  int sasa_warps = 2;     // warps (atoms) per k_sasa block
   bool tuned = false;
   int64_t tune_frames = 0;
   double tune_ms[12] = {};  // candidate times of the tuning run (k_pairs, k_sasa, k_psi shapes)
